@@ -1,0 +1,118 @@
+"""Pin the oracle restatement (oracle/gsknn_oracle.c) to outputs of the reference library
+compiled from its own sources (fixtures in tests/golden/, made by tests/golden/make_golden.py).
+
+The restated reference routines must match bit for bit; the tie-resolved exact oracle must
+agree with the reference's outputs modulo ties at the k-th boundary."""
+import numpy as np
+import pytest
+
+from knn_check import compare_sets, exact_dists, is_maxheap, sorted_rows
+from rnn_b200 import workloads as W
+
+REF_CASES = ["ref_d_basic", "ref_s_basic", "ref_d_prefill", "ref_s_gmm_d64", "ref_d_ties",
+             "ref_s_ties", "ref_d_few", "ref_d_odd", "ref_s_odd", "ref_d_one"]
+
+
+@pytest.mark.parametrize("case", REF_CASES)
+def test_gsknn_ref_bit_exact(oracle, golden, case):
+    g = golden(case)
+    D, I = g["Din"].copy(), g["Iin"].copy()
+    oracle.gsknn_ref(int(g["k"]), g["X"], g["X2"], g["alpha"], g["X"], g["X2"], g["beta"], D, I)
+    assert np.array_equal(D, g["Dout"])
+    assert np.array_equal(I, g["Iout"])
+    assert oracle.is_maxheap(D)
+
+
+@pytest.mark.parametrize("case", REF_CASES + ["ref_d_stl"])
+def test_exact_oracle_matches_reference_modulo_ties(oracle, golden, case):
+    g = golden(case)
+    k, X, X2 = int(g["k"]), g["X"], g["X2"]
+    De, Ie = oracle.knn_exact(k, X, X2, g["alpha"], X, X2, g["beta"], g["Din"], g["Iin"],
+                              clamp=False)
+    # Reference distances are computed in the working precision; ties at the k-th boundary
+    # are resolved differently (later candidate vs lower index), so compare modulo a band of
+    # the working precision's rounding.
+    eps = 1e-12 if X.dtype == np.float64 else 2e-5
+    band = eps * np.maximum(1.0, np.abs(De).max(axis=1)) * 8
+    beta = g["beta"]
+    eq, bad = compare_sets(g["Iout"], Ie, De, band,
+                           dist_of=lambda j, ids: exact_dists(X, beta[j], ids, X2))
+    assert not bad, f"{case}: {len(bad)} rows differ beyond ties: {bad[:5]}"
+    Ds, _ = sorted_rows(g["Dout"].astype(np.float64), g["Iout"])
+    fin = np.isfinite(De) & (De < 1e30)
+    rel = np.abs(Ds[fin] - De[fin]) / np.maximum(np.abs(De[fin]), 1.0)
+    assert rel.max(initial=0.0) <= eps * 64
+
+
+def test_heapselect_bit_exact(oracle, golden):
+    g = golden("heapselect")
+    for tag in ("d", "s"):
+        D, I = g[f"Din_{tag}"].copy(), g[f"Iin_{tag}"].copy()
+        oracle.heap_select(g[f"keys_{tag}"], g[f"alpha_{tag}"], D, I)
+        assert np.array_equal(D, g[f"Dout_{tag}"])
+        assert np.array_equal(I, g[f"Iout_{tag}"])
+
+
+def test_dgssq2nrm_bit_exact(oracle, golden):
+    g = golden("dgssq2nrm_d300")
+    C = oracle.dgssq2nrm(g["X"], g["X2"], g["amap"], g["X"], g["X2"], g["bmap"],
+                         ldc=int(g["ldc"]))
+    assert np.array_equal(C[:, :g["amap"].size], g["C"])
+
+
+def test_var3_4ary_bit_exact(oracle, golden):
+    g = golden("var3_k600")
+    k, X, X2, beta = int(g["k"]), g["X"], g["X2"], g["beta"]
+    D, I = g["Din"].copy(), g["Iin"].copy()
+    for c, m in enumerate(g["ms"]):
+        alpha = np.ascontiguousarray(g["alphas"][c][:m])
+        oracle.dgsknn_var3(k, X, X2, alpha, X, X2, beta, D, I)
+        assert np.array_equal(D, g["Douts"][c]), f"call {c}"
+        assert np.array_equal(I, g["Iouts"][c]), f"call {c}"
+        assert oracle.is_maxheap4(D, I, k)
+
+
+@pytest.mark.parametrize("case", ["opt_d_merge", "opt_s_gmm", "opt_d_d300", "opt_s_d300"])
+def test_optimized_reference_vs_exact_oracle(oracle, golden, case):
+    """The reference's optimized dgsknn/sgsknn (heap_t path, successive merging calls) agrees
+    with the exact oracle merged call by call."""
+    g = golden(case)
+    k, X, X2, beta = int(g["k"]), g["X"], g["X2"], g["beta"]
+    D, I = g["Din"], g["Iin"]
+    eps = 1e-12 if X.dtype == np.float64 else 2e-5
+    for c in range(g["alphas"].shape[0]):
+        De, Ie = oracle.knn_exact(k, X, X2, g["alphas"][c], X, X2, beta, D, I, clamp=True)
+        got_D, got_I = g["Douts"][c], g["Iouts"][c]
+        assert is_maxheap(got_D)
+        band = eps * np.maximum(1.0, np.abs(De).max(axis=1)) * 64
+        eq, bad = compare_sets(got_I, Ie, De, band,
+                               dist_of=lambda j, ids: exact_dists(X, beta[j], ids, X2))
+        assert not bad, f"{case} call {c}: rows {bad[:5]}"
+        D, I = got_D, got_I
+
+
+def test_config1_full_size(oracle, golden):
+    """Config 1 (dgsknn f64, N=8192, d=32, m=n=4096, k=16, two merging calls)."""
+    g = golden("config1_dgsknn")
+    p, alpha2 = W.config1(int(g["seed"]))
+    import hashlib
+    h = hashlib.sha256()
+    for a in (p.X, p.X2, p.alpha, p.beta, alpha2):
+        h.update(np.ascontiguousarray(a).tobytes())
+    assert h.hexdigest() == str(g["input_sha256"]), "workload generator drifted"
+    # restated dgsknn_ref: bit-exact over both calls
+    D, I = p.empty_heap(1.79e308)
+    oracle.gsknn_ref(p.k, p.X, p.X2, p.alpha, p.X, p.X2, p.beta, D, I)
+    assert np.array_equal(D, g["Dref1"]) and np.array_equal(I, g["Iref1"])
+    oracle.gsknn_ref(p.k, p.X, p.X2, alpha2, p.X, p.X2, p.beta, D, I)
+    assert np.array_equal(D, g["Dref2"]) and np.array_equal(I, g["Iref2"])
+    # optimized dgsknn vs the exact oracle: identical index sets, distances within 1e-12
+    D0, I0 = p.empty_heap(1.79e308)
+    De1, Ie1 = oracle.knn_exact(p.k, p.X, p.X2, p.alpha, p.X, p.X2, p.beta, D0, I0)
+    De2, Ie2 = oracle.knn_exact(p.k, p.X, p.X2, alpha2, p.X, p.X2, p.beta, De1, Ie1)
+    for (Dg, Ig, De, Ie) in ((g["D1"], g["I1"], De1, Ie1), (g["D2"], g["I2"], De2, Ie2)):
+        assert is_maxheap(Dg)
+        eq, bad = compare_sets(Ig, Ie, De, np.full(p.n, 0.0))
+        assert not bad
+        Ds, _ = sorted_rows(Dg, Ig)
+        assert np.max(np.abs(Ds - De) / np.maximum(De, 1e-300)) <= 1e-12
