@@ -1,0 +1,187 @@
+/*
+ * gsknn.h -- public C ABI of the B200 GSKNN library (libgsknn.so).
+ *
+ * Drop-in for the GSKNN C API (ChenhanYu/rnn, include/gsknn.h): every prototype, constant and
+ * struct layout of the reference header is kept, with the same argument meaning, so a program
+ * or binding built against the reference links against this library unchanged. Behind it the
+ * fused distance + k-selection work runs as CUDA kernels on one B200 (sm_100a).
+ *
+ * Argument convention of the reference (frame/gsknn.c:1106-1184):
+ *   dgsknn/sgsknn(m, n, k, r, XA, XA2, alpha, XB, XB2, beta, heap)
+ *     m  = number of candidate points alpha[0..m) of table XA (norms XA2)
+ *     n  = number of query points beta[0..n) of table XB (norms XB2) = heap rows
+ *     k  = dimension d, r = number of neighbours
+ *   *_var1(m, n, k, r, XA, XA2, amap, XB, XB2, bmap, D, I) have the roles swapped:
+ *     m/XA/amap are the queries (heap rows), n/XB/bmap the candidates, D/I are m x r.
+ * Tables are row-major (row i of table X is X[i*d .. i*d+d)); norms are squared 2-norms indexed
+ * by global point id; D/I rows are max-heaps updated in place, so repeated calls merge.
+ *
+ * All pointers of the reference API are host pointers; each call copies what it needs to the
+ * GPU and back, and returns when D/I are updated. Extensions (prefixed gsknn_) take device
+ * pointers and a CUDA stream for resident data.
+ *
+ * Behavioural notes against the reference:
+ *   - ties at the k-th distance go to the lower point id (the reference keeps the later
+ *     candidate), so results equal the reference's as index sets modulo exact ties;
+ *   - squared distances are clamped at 0 in both precisions (the reference clamps in its
+ *     double micro-kernel only, kernels/x86_64/sandybridge/rnn_r_int_d8x4_row.c:373-382);
+ *   - errors never exit() the process: the call returns with D/I untouched and the status is
+ *     available from gsknn_last_error().
+ */
+#ifndef GSKNN_B200_H
+#define GSKNN_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#include <math.h>
+#include <stddef.h>
+
+/* include/gsknn.h:46-47 of the reference */
+#define KNN_VAR_THRES 512
+#define KNN_HEAP_OFFSET 3
+
+typedef unsigned long long dim_t;
+
+/* include/gsknn.h:51-59 */
+typedef enum { KNN_2NORM, KNN_1NORM } knn_type;
+typedef enum { KNN_DOUBLE, KNN_SINGLE } knn_prec;
+
+/* include/gsknn.h:61-73: micro-kernel side channel. Kept for layout compatibility only; the
+ * CUDA kernels take their parameters by value and never read it. */
+struct aux_s {
+  double *b_next;
+  float *b_next_s;
+  int *I;
+  double *D;
+  float *D_s;
+  int ldr;
+  char *flag;
+  int pc;
+  int m;
+  int n;
+};
+typedef struct aux_s aux_t;
+
+/* include/gsknn.h:75-88: a set of m neighbour lists of k entries, row stride ldk.
+ * d = 2 for binary heaps; d = 4 for the 4-ary heaps with a 3-slot header that heapCreate_d
+ * builds when k > KNN_VAR_THRES (D = [ro,0,0 | heap], I = [k, filled, ldk | heap]). */
+struct heap_s {
+  int m;
+  int k;
+  int ldk;
+  int d;
+  double ro;
+  double *D;
+  float ro_s;
+  float *D_s;
+  int *I;
+  knn_type type;
+  knn_prec prec;
+};
+typedef struct heap_s heap_t;
+
+/* ---- fused kNN: replaces frame/gsknn.c:1106-1135 (sgsknn) and 1138-1184 (dgsknn) ---- */
+void sgsknn(int m, int n, int k, int r, float *XA, float *XA2, int *alpha, float *XB,
+            float *XB2, int *beta, heap_t *heap);
+void dgsknn(int m, int n, int k, int r, double *XA, double *XA2, int *alpha, double *XB,
+            double *XB2, int *beta, heap_t *heap);
+
+/* ---- replaces frame/gsknn.c:665-880 (sgsknn_var1) and 883-1103 (dgsknn_var1); the entry
+ *      points python/gsknn.py:79-92 and 169-182 bind ---- */
+void sgsknn_var1(int m, int n, int k, int r, float *XA, float *XA2, int *alpha, float *XB,
+                 float *XB2, int *beta, float *D, int *I);
+void dgsknn_var1(int m, int n, int k, int r, double *XA, double *XA2, int *alpha, double *XB,
+                 double *XB2, int *beta, double *D, int *I);
+
+/* ---- replaces frame/gsknn.c:597-659: large-k double path over heap_t storage (4-ary heaps
+ *      with header when heap->d == 4, binary heaps otherwise) ---- */
+void dgsknn_var3(int m, int n, int k, int r, double *XA, double *XA2, int *amap, double *XB,
+                 double *XB2, int *bmap, heap_t *heap);
+
+/* ---- replaces frame/gsknn.c:481-594: C[j*ldc + i] = |XA[amap[i]] - XB[bmap[j]]|^2 computed
+ *      as -2<a,b> + XA2[amap[i]] + XB2[bmap[j]] (no clamp), i < m, j < n ---- */
+void dgssq2nrm(int m, int n, int k, double *XA, double *XA2, int *amap, double *XB,
+               double *XB2, int *bmap, double *C, int ldc);
+
+/* ---- host utilities: replace frame/gsknn_util.c:53-133 and frame/gsknn_heap.c:52-337 ---- */
+double *gsknn_malloc_aligned(int m, int n, int size);
+heap_t *heapCreate_s(int m, int k, float ro);
+heap_t *heapCreate_d(int m, int k, double ro);
+void heapFree_s(heap_t *heap);
+void heapFree_d(heap_t *heap);
+heap_t *heapAttach_s(int m, int k, float *D, int *I);
+heap_t *heapAttach_d(int m, int k, double *D, int *I);
+void heapSelect_s(int m, int r, float *x, int *alpha, float *D, int *I);
+void heapSelect_d(int m, int r, double *x, int *alpha, double *D, int *I);
+/* Declared by the reference (include/gsknn.h:236-243) without a definition; here it is the
+ * 4-ary header-heap select that dgsknn_var3 performs per row. */
+void heapSelect_dheap(int m, int k, double *key, int *val, double *D, int *I);
+void swap_float(float *x, int i, int j);
+void swap_double(double *x, int i, int j);
+void swap_int(int *I, int i, int j);
+void bubbleSort_s(int n, float *D, int *I);
+void bubbleSort_d(int n, double *D, int *I);
+
+/* ---- reference-algorithm entry points: replace frame/gsknn_ref.c:63-162 (the
+ *      python/gsknn.py:34 and 124 bindings). They run the unfused GPU path (explicit distance
+ *      block, then per-row heap selection) with the reference oracle's D/I convention
+ *      (n rows of r, m candidates on the XA/alpha side). ---- */
+void sgsknn_ref(int m, int n, int k, int r, float *XA, float *XA2, int *alpha, float *XB,
+                float *XB2, int *beta, float *D, int *I);
+void dgsknn_ref(int m, int n, int k, int r, double *XA, double *XA2, int *alpha, double *XB,
+                double *XB2, int *beta, double *D, int *I);
+
+/* =====================================================================================
+ * Extensions (no counterpart in the reference)
+ * ===================================================================================== */
+
+/* Status of the calling thread's last call: 0 = ok, 1 = early return (m, n, d or k was 0,
+ * as frame/gsknn.c:910-913), >= 2 = error; the string says what failed. */
+int gsknn_last_error(void);
+const char *gsknn_last_error_string(void);
+
+/* Arithmetic of the float path of sgsknn / sgsknn_var1 / gsknn_s_device:
+ *   GSKNN_MODE_FP32 -- CUDA-core FP32 distances;
+ *   GSKNN_MODE_TF32, GSKNN_MODE_BF16 -- tensor-core distances with an FP64 re-rank of every
+ *     candidate within the rounding bound of the k-th distance (exact index sets);
+ *   GSKNN_MODE_AUTO -- the faster exact choice for the problem shape (default). */
+#define GSKNN_MODE_AUTO 0
+#define GSKNN_MODE_FP32 1
+#define GSKNN_MODE_TF32 2
+#define GSKNN_MODE_BF16 3
+int gsknn_set_mode(int mode);
+int gsknn_get_mode(void);
+
+/* Device-pointer entry points, asynchronous on `stream` (a cudaStream_t; NULL = the legacy
+ * default stream). Roles as in dgsknn: m candidates alpha[] of table XA (nA rows), n queries
+ * beta[] of table XB (nB rows); D/I are n rows of stride ldD holding binary max-heaps of k
+ * entries, updated in place. Indices outside a table are reported as an error (not read).
+ * Scratch memory is taken from a per-(device, stream) cache owned by the library.
+ * Returns 0 when the work was enqueued; call gsknn_stream_status(stream) after the stream has
+ * drained to learn whether device-side checks failed. */
+int gsknn_s_device(int m, int n, int d, int k, const float *XA, const float *XA2, long long nA,
+                   const int *alpha, const float *XB, const float *XB2, long long nB,
+                   const int *beta, float *D, int *I, int ldD, void *stream);
+int gsknn_d_device(int m, int n, int d, int k, const double *XA, const double *XA2,
+                   long long nA, const int *alpha, const double *XB, const double *XB2,
+                   long long nB, const int *beta, double *D, int *I, int ldD, void *stream);
+
+/* Synchronises `stream` and returns the device-side status of the last call enqueued on it. */
+int gsknn_stream_status(void *stream);
+
+/* Launch tracing: while enabled, every kernel the library launches is bracketed by CUDA events
+ * on its stream. gsknn_trace_read() waits for the recorded launches, writes a JSON object
+ * {"kernel": {"launches": n, "ms": total}, ...} into buf and clears the record; it returns the
+ * number of launches read. */
+void gsknn_trace_enable(int on);
+int gsknn_trace_read(char *buf, int len);
+
+/* Frees the library's cached device scratch memory of the current device. */
+void gsknn_release_workspace(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GSKNN_B200_H */

@@ -1,0 +1,497 @@
+// gsknn_api.cu -- the C ABI of libgsknn.so (declared in include/gsknn.h).
+//
+// Host-pointer entry points (the reference API) copy the referenced row range of each point
+// table, the index lists and the heap rows to the GPU, run the device pipeline, copy D/I back
+// and return when done. Device-pointer entry points (gsknn_*_device) enqueue the same pipeline
+// on a caller stream. Scratch memory comes from a cache keyed by (device, stream, slot).
+#include "gsknn.h"
+#include "knn_internal.h"
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+namespace gsknn {
+
+// ------------------------------------------------------------------------------------------
+// status
+// ------------------------------------------------------------------------------------------
+static thread_local int t_status = 0;
+static thread_local char t_msg[512] = "ok";
+
+int set_status(int code, const char *fmt, ...) {
+  t_status = code;
+  if (fmt) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(t_msg, sizeof(t_msg), fmt, ap);
+    va_end(ap);
+  } else {
+    snprintf(t_msg, sizeof(t_msg), "%s", code == 0 ? "ok" : "error");
+  }
+  return code;
+}
+
+#define CU(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return set_status(e_ == cudaErrorMemoryAllocation ? GSKNN_ERR_NOMEM : GSKNN_ERR_CUDA, \
+                        "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__,  \
+                        __LINE__);                                                        \
+  } while (0)
+
+// ------------------------------------------------------------------------------------------
+// scratch cache
+// ------------------------------------------------------------------------------------------
+enum Slot { SLOT_KERNEL = 0, SLOT_STATUS, SLOT_HQTAB, SLOT_HCTAB, SLOT_HQNRM, SLOT_HCNRM,
+            SLOT_HQIDX, SLOT_HCIDX, SLOT_HD, SLOT_HI, SLOT_AUX };
+
+struct Buf {
+  void *p = nullptr;
+  size_t n = 0;
+};
+static std::mutex g_mu;
+static std::map<std::tuple<int, uintptr_t, int>, Buf> g_bufs;
+
+static cudaError_t scratch(int slot, size_t bytes, cudaStream_t st, void **out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(g_mu);
+  Buf &b = g_bufs[std::make_tuple(dev, (uintptr_t)st, slot)];
+  if (b.n < bytes) {
+    if (b.p) {
+      e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) return e;
+      cudaFree(b.p);
+      b.p = nullptr;
+      b.n = 0;
+    }
+    size_t nb = std::max(bytes, (size_t)4096);
+    e = cudaMalloc(&b.p, nb);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      return e;
+    }
+    b.n = nb;
+  }
+  *out = b.p;
+  return cudaSuccess;
+}
+
+static void release_all_for_device(int dev) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  for (auto it = g_bufs.begin(); it != g_bufs.end();) {
+    if (std::get<0>(it->first) == dev) {
+      cudaStreamSynchronize((cudaStream_t)std::get<1>(it->first));
+      cudaFree(it->second.p);
+      it = g_bufs.erase(it);
+    } else {
+      ++it;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// launch tracing: CUDA events around every kernel launch of the library, on its stream
+// ------------------------------------------------------------------------------------------
+struct TraceRec {
+  const char *name;
+  cudaEvent_t a, b;
+};
+static std::mutex g_tmu;
+static bool g_trace = false;
+static std::vector<TraceRec> g_recs;
+static std::vector<cudaEvent_t> g_evpool;
+
+static cudaEvent_t ev_get() {
+  if (!g_evpool.empty()) {
+    cudaEvent_t e = g_evpool.back();
+    g_evpool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+struct TraceScope {
+  const char *name;
+  cudaStream_t st;
+  cudaEvent_t a = nullptr;
+  TraceScope(const char *n, cudaStream_t s) : name(n), st(s) {
+    if (!g_trace) return;
+    std::lock_guard<std::mutex> lk(g_tmu);
+    a = ev_get();
+    cudaEventRecord(a, st);
+  }
+  ~TraceScope() {
+    if (!a) return;
+    std::lock_guard<std::mutex> lk(g_tmu);
+    cudaEvent_t b = ev_get();
+    cudaEventRecord(b, st);
+    g_recs.push_back({name, a, b});
+  }
+};
+
+static cudaStream_t host_stream() {
+  static thread_local std::map<int, cudaStream_t> streams;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  auto it = streams.find(dev);
+  if (it != streams.end()) return it->second;
+  cudaStream_t s = nullptr;
+  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) s = nullptr;
+  streams[dev] = s;
+  return s;
+}
+
+static int sm_count() {
+  int dev = 0, n = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n > 0 ? n : 148;
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Number of candidate splits per query tile: balances the waves of CTAs over the SMs.
+static int choose_splits(int qtiles, int rtiles, int slots) {
+  int best_s = 1;
+  double best = 1e300;
+  const int smax = std::min(rtiles, 64);
+  for (int s = 1; s <= smax; s++) {
+    const long long items = (long long)qtiles * s;
+    const double waves = (double)((items + slots - 1) / slots);
+    const double cost = waves / s * (1.0 + 0.004 * s);  // small per-split merge cost
+    if (cost < best - 1e-12) {
+      best = cost;
+      best_s = s;
+    }
+  }
+  return best_s;
+}
+
+// ------------------------------------------------------------------------------------------
+// device pipeline: pack -> fused select -> finalize (queries = heap rows)
+// ------------------------------------------------------------------------------------------
+template <typename T>
+int knn_device(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, long long nrows_q,
+               const int *qidx, const T *Xc, const T *Xc2, long long nrows_c, const int *cidx,
+               T *D, int *I, int ldD, cudaStream_t st) {
+  if (nq == 0 || nc == 0 || d == 0 || k == 0)
+    return set_status(GSKNN_EARLY_RETURN, "early return: m, n, d or k is 0");
+  if (nq < 0 || nc < 0 || d < 0 || k < 0 || ldD < k)
+    return set_status(GSKNN_ERR_ARG, "invalid sizes (n=%d m=%d d=%d k=%d ldD=%d)", nq, nc, d,
+                      k, ldD);
+  if (!Xq || !Xq2 || !qidx || !Xc || !Xc2 || !cidx || !D || !I)
+    return set_status(GSKNN_ERR_ARG, "null pointer argument");
+  const SimtGeom g = simt_geometry<T>(k);
+  if (g.kp == 0)
+    return set_status(GSKNN_ERR_UNSUPPORTED, "k=%d exceeds the fused kernel's list size", k);
+
+  const int nkc = (d + g.dk - 1) / g.dk;
+  const int qtiles = (nq + g.bq - 1) / g.bq;
+  const int rtiles = (nc + g.br - 1) / g.br;
+  const int S = choose_splits(qtiles, rtiles, sm_count());
+  const int tps = (rtiles + S - 1) / S;
+
+  size_t off = 0;
+  auto take = [&](size_t bytes) { size_t o = off; off = align256(off + bytes); return o; };
+  const size_t oA = take((size_t)qtiles * nkc * g.dk * g.bq * sizeof(T));
+  const size_t oB = take((size_t)rtiles * nkc * g.dk * g.br * sizeof(T));
+  const size_t oQN = take((size_t)qtiles * g.bq * sizeof(T));
+  const size_t oCN = take((size_t)rtiles * g.br * sizeof(T));
+  const size_t oCI = take((size_t)rtiles * g.br * 4);
+  const size_t oPD = take((size_t)S * nq * k * sizeof(T));
+  const size_t oPI = take((size_t)S * nq * k * 4);
+  void *ws = nullptr, *stv = nullptr;
+  CU(scratch(SLOT_KERNEL, off, st, &ws));
+  CU(scratch(SLOT_STATUS, 256, st, &stv));
+  char *base = static_cast<char *>(ws);
+  int *status = static_cast<int *>(stv);
+  CU(cudaMemsetAsync(status, 0, sizeof(int), st));
+
+  T *Apack = reinterpret_cast<T *>(base + oA);
+  T *Bpack = reinterpret_cast<T *>(base + oB);
+  T *qn = reinterpret_cast<T *>(base + oQN);
+  T *cn = reinterpret_cast<T *>(base + oCN);
+  uint32_t *cid = reinterpret_cast<uint32_t *>(base + oCI);
+  T *partD = reinterpret_cast<T *>(base + oPD);
+  uint32_t *partI = reinterpret_cast<uint32_t *>(base + oPI);
+
+  {
+    TraceScope ts("pack_panels", st);
+    CU(launch_pack<T>(Xq, Xq2, d, nrows_q, qidx, nq, g.bq, g.dk, nkc, Apack, qn, nullptr,
+                      status, st));
+  }
+  {
+    TraceScope ts("pack_panels", st);
+    CU(launch_pack<T>(Xc, Xc2, d, nrows_c, cidx, nc, g.br, g.dk, nkc, Bpack, cn, cid, status,
+                      st));
+  }
+  SimtArgs<T> sa{};
+  sa.Apack = Apack; sa.Bpack = Bpack; sa.qn = qn; sa.cn = cn; sa.cid = cid;
+  sa.Din = D; sa.ldD = ldD; sa.Q = nq; sa.k = k; sa.nkc = nkc;
+  sa.ntiles_r = rtiles; sa.tiles_per_split = tps; sa.partD = partD; sa.partI = partI;
+  {
+    TraceScope ts("fused_knn_simt", st);
+    CU(launch_simt<T>(sa, g.kp, qtiles, S, st));
+  }
+  FinalizeArgs<T> fa{};
+  fa.Din = D; fa.Iin = I; fa.ldD = ldD; fa.Q = nq; fa.k = k; fa.S = S;
+  fa.partD = partD; fa.partI = partI; fa.Dout = D; fa.Iout = I;
+  {
+    TraceScope ts("finalize_heap", st);
+    CU(launch_finalize<T>(fa, g.kp, st));
+  }
+  return set_status(GSKNN_OK, nullptr);
+}
+
+// Reads back the device status word of `st` (after synchronising it).
+static int device_status(cudaStream_t st) {
+  void *stv = nullptr;
+  CU(scratch(SLOT_STATUS, 256, st, &stv));
+  CU(cudaStreamSynchronize(st));
+  int h = 0;
+  CU(cudaMemcpy(&h, stv, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h == GSKNN_ERR_INDEX)
+    return set_status(GSKNN_ERR_INDEX, "an alpha/beta index lies outside its point table");
+  if (h == GSKNN_ERR_TIMEOUT)
+    return set_status(GSKNN_ERR_TIMEOUT, "a bounded device-side wait gave up");
+  if (h != 0) return set_status(h, "device-side error %d", h);
+  return GSKNN_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// host-pointer path
+// ------------------------------------------------------------------------------------------
+static bool index_range(const int *idx, int n, int *lo, int *hi) {
+  int a = idx[0], b = idx[0];
+  for (int i = 1; i < n; i++) {
+    const int v = idx[i];
+    a = v < a ? v : a;
+    b = v > b ? v : b;
+  }
+  *lo = a;
+  *hi = b;
+  return a >= 0;
+}
+
+template <typename T>
+int knn_host(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, const int *qidx,
+             const T *Xc, const T *Xc2, const int *cidx, T *D, int *I, int ldD) {
+  if (nq == 0 || nc == 0 || d == 0 || k == 0)
+    return set_status(GSKNN_EARLY_RETURN, "early return: m, n, d or k is 0");
+  if (nq < 0 || nc < 0 || d < 0 || k < 0 || ldD < k)
+    return set_status(GSKNN_ERR_ARG, "invalid sizes");
+  if (!Xq || !Xq2 || !qidx || !Xc || !Xc2 || !cidx || !D || !I)
+    return set_status(GSKNN_ERR_ARG, "null pointer argument");
+  int qlo, qhi, clo, chi;
+  if (!index_range(qidx, nq, &qlo, &qhi) || !index_range(cidx, nc, &clo, &chi))
+    return set_status(GSKNN_ERR_INDEX, "negative point index");
+  cudaStream_t st = host_stream();
+  const bool same = (Xq == Xc) && (Xq2 == Xc2);
+  if (same) {
+    qlo = clo = std::min(qlo, clo);
+    qhi = chi = std::max(qhi, chi);
+  }
+  auto copy_table = [&](int slot_t, int slot_n, const T *X, const T *X2, int lo, int hi,
+                        const T **dX, const T **dX2) -> int {
+    const size_t rows = (size_t)(hi - lo + 1);
+    void *pt = nullptr, *pn = nullptr;
+    CU(scratch(slot_t, rows * d * sizeof(T), st, &pt));
+    CU(scratch(slot_n, rows * sizeof(T), st, &pn));
+    CU(cudaMemcpyAsync(pt, X + (size_t)lo * d, rows * d * sizeof(T), cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(pn, X2 + lo, rows * sizeof(T), cudaMemcpyHostToDevice, st));
+    // offset so that global row ids index the copied range directly
+    *dX = static_cast<const T *>(pt) - (size_t)lo * d;
+    *dX2 = static_cast<const T *>(pn) - lo;
+    return 0;
+  };
+  const T *dXq, *dXq2, *dXc, *dXc2;
+  int rc = copy_table(SLOT_HQTAB, SLOT_HQNRM, Xq, Xq2, qlo, qhi, &dXq, &dXq2);
+  if (rc) return rc;
+  if (same) {
+    dXc = dXq;
+    dXc2 = dXq2;
+  } else {
+    rc = copy_table(SLOT_HCTAB, SLOT_HCNRM, Xc, Xc2, clo, chi, &dXc, &dXc2);
+    if (rc) return rc;
+  }
+  void *pqi, *pci, *pD, *pI;
+  CU(scratch(SLOT_HQIDX, (size_t)nq * 4, st, &pqi));
+  CU(scratch(SLOT_HCIDX, (size_t)nc * 4, st, &pci));
+  CU(scratch(SLOT_HD, (size_t)nq * ldD * sizeof(T), st, &pD));
+  CU(scratch(SLOT_HI, (size_t)nq * ldD * 4, st, &pI));
+  CU(cudaMemcpyAsync(pqi, qidx, (size_t)nq * 4, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(pci, cidx, (size_t)nc * 4, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(pD, D, (size_t)nq * ldD * sizeof(T), cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(pI, I, (size_t)nq * ldD * 4, cudaMemcpyHostToDevice, st));
+  rc = knn_device<T>(nq, nc, d, k, dXq, dXq2, (long long)qhi + 1, static_cast<int *>(pqi),
+                     dXc, dXc2, (long long)chi + 1, static_cast<int *>(pci),
+                     static_cast<T *>(pD), static_cast<int *>(pI), ldD, st);
+  if (rc != GSKNN_OK) {
+    cudaStreamSynchronize(st);
+    return rc;
+  }
+  rc = device_status(st);
+  if (rc != GSKNN_OK) return rc;
+  CU(cudaMemcpyAsync(D, pD, (size_t)nq * ldD * sizeof(T), cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(I, pI, (size_t)nq * ldD * 4, cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  return set_status(GSKNN_OK, nullptr);
+}
+
+static int g_mode = GSKNN_MODE_AUTO;
+
+}  // namespace gsknn
+
+using namespace gsknn;
+
+// ==========================================================================================
+// C ABI
+// ==========================================================================================
+extern "C" {
+
+int gsknn_last_error(void) { return t_status; }
+const char *gsknn_last_error_string(void) { return t_msg; }
+
+int gsknn_set_mode(int mode) {
+  if (mode < GSKNN_MODE_AUTO || mode > GSKNN_MODE_BF16)
+    return set_status(GSKNN_ERR_ARG, "unknown mode %d", mode);
+  g_mode = mode;
+  return set_status(GSKNN_OK, nullptr);
+}
+int gsknn_get_mode(void) { return g_mode; }
+
+int gsknn_s_device(int m, int n, int d, int k, const float *XA, const float *XA2, long long nA,
+                   const int *alpha, const float *XB, const float *XB2, long long nB,
+                   const int *beta, float *D, int *I, int ldD, void *stream) {
+  return knn_device<float>(n, m, d, k, XB, XB2, nB, beta, XA, XA2, nA, alpha, D, I, ldD,
+                           (cudaStream_t)stream);
+}
+
+int gsknn_d_device(int m, int n, int d, int k, const double *XA, const double *XA2,
+                   long long nA, const int *alpha, const double *XB, const double *XB2,
+                   long long nB, const int *beta, double *D, int *I, int ldD, void *stream) {
+  return knn_device<double>(n, m, d, k, XB, XB2, nB, beta, XA, XA2, nA, alpha, D, I, ldD,
+                            (cudaStream_t)stream);
+}
+
+int gsknn_stream_status(void *stream) { return device_status((cudaStream_t)stream); }
+
+void gsknn_trace_enable(int on) {
+  std::lock_guard<std::mutex> lk(g_tmu);
+  g_trace = on != 0;
+}
+
+int gsknn_trace_read(char *buf, int len) {
+  std::lock_guard<std::mutex> lk(g_tmu);
+  struct Acc { int n = 0; double ms = 0.0; };
+  std::map<std::string, Acc> acc;
+  int total = 0;
+  for (auto &r : g_recs) {
+    cudaEventSynchronize(r.b);
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+      Acc &x = acc[r.name];
+      x.n++;
+      x.ms += ms;
+    }
+    g_evpool.push_back(r.a);
+    g_evpool.push_back(r.b);
+    total++;
+  }
+  g_recs.clear();
+  std::string out = "{";
+  bool first = true;
+  for (auto &kv : acc) {
+    char tmp[256];
+    snprintf(tmp, sizeof(tmp), "%s\"%s\": {\"launches\": %d, \"ms\": %.6f}", first ? "" : ", ",
+             kv.first.c_str(), kv.second.n, kv.second.ms);
+    out += tmp;
+    first = false;
+  }
+  out += "}";
+  if (buf && len > 0) snprintf(buf, (size_t)len, "%s", out.c_str());
+  return total;
+}
+
+void gsknn_release_workspace(void) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  release_all_for_device(dev);
+}
+
+// ---- reference entry points (frame/gsknn.c) ----
+void sgsknn_var1(int m, int n, int k, int r, float *XA, float *XA2, int *alpha, float *XB,
+                 float *XB2, int *beta, float *D, int *I) {
+  knn_host<float>(m, n, k, r, XA, XA2, alpha, XB, XB2, beta, D, I, r);
+}
+
+void dgsknn_var1(int m, int n, int k, int r, double *XA, double *XA2, int *alpha, double *XB,
+                 double *XB2, int *beta, double *D, int *I) {
+  knn_host<double>(m, n, k, r, XA, XA2, alpha, XB, XB2, beta, D, I, r);
+}
+
+void sgsknn(int m, int n, int k, int r, float *XA, float *XA2, int *alpha, float *XB,
+            float *XB2, int *beta, heap_t *heap) {
+  if (!heap) {
+    set_status(GSKNN_ERR_ARG, "null heap");
+    return;
+  }
+  knn_host<float>(n, m, k, r, XB, XB2, beta, XA, XA2, alpha, heap->D_s, heap->I, heap->ldk);
+}
+
+void dgsknn(int m, int n, int k, int r, double *XA, double *XA2, int *alpha, double *XB,
+            double *XB2, int *beta, heap_t *heap) {
+  if (!heap) {
+    set_status(GSKNN_ERR_ARG, "null heap");
+    return;
+  }
+  if (r > KNN_VAR_THRES) {
+    dgsknn_var3(m, n, k, r, XA, XA2, alpha, XB, XB2, beta, heap);
+    return;
+  }
+  knn_host<double>(n, m, k, r, XB, XB2, beta, XA, XA2, alpha, heap->D, heap->I, heap->ldk);
+}
+
+void dgsknn_var3(int m, int n, int k, int r, double *XA, double *XA2, int *amap, double *XB,
+                 double *XB2, int *bmap, heap_t *heap) {
+  (void)m; (void)n; (void)k; (void)r; (void)XA; (void)XA2; (void)amap; (void)XB; (void)XB2;
+  (void)bmap; (void)heap;
+  set_status(GSKNN_ERR_UNSUPPORTED, "dgsknn_var3: large-k path not built yet");
+}
+
+void dgssq2nrm(int m, int n, int k, double *XA, double *XA2, int *amap, double *XB,
+               double *XB2, int *bmap, double *C, int ldc) {
+  (void)m; (void)n; (void)k; (void)XA; (void)XA2; (void)amap; (void)XB; (void)XB2; (void)bmap;
+  (void)C; (void)ldc;
+  set_status(GSKNN_ERR_UNSUPPORTED, "dgssq2nrm: not built yet");
+}
+
+void sgsknn_ref(int m, int n, int k, int r, float *XA, float *XA2, int *alpha, float *XB,
+                float *XB2, int *beta, float *D, int *I) {
+  (void)m; (void)n; (void)k; (void)r; (void)XA; (void)XA2; (void)alpha; (void)XB; (void)XB2;
+  (void)beta; (void)D; (void)I;
+  set_status(GSKNN_ERR_UNSUPPORTED, "sgsknn_ref: not built yet");
+}
+
+void dgsknn_ref(int m, int n, int k, int r, double *XA, double *XA2, int *alpha, double *XB,
+                double *XB2, int *beta, double *D, int *I) {
+  (void)m; (void)n; (void)k; (void)r; (void)XA; (void)XA2; (void)alpha; (void)XB; (void)XB2;
+  (void)beta; (void)D; (void)I;
+  set_status(GSKNN_ERR_UNSUPPORTED, "dgsknn_ref: not built yet");
+}
+
+}  // extern "C"

@@ -1,0 +1,66 @@
+// knn_internal.h -- internal interfaces between the C-ABI layer and the CUDA kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+// Status codes (also reported through gsknn_last_error()).
+#define GSKNN_OK 0
+#define GSKNN_EARLY_RETURN 1     // m, n, d or k was 0: nothing to do (frame/gsknn.c:910-913)
+#define GSKNN_ERR_ARG 2          // invalid argument
+#define GSKNN_ERR_CUDA 3         // a CUDA runtime call failed
+#define GSKNN_ERR_INDEX 4        // an alpha/beta entry lies outside the point table
+#define GSKNN_ERR_UNSUPPORTED 5  // size outside what this build supports
+#define GSKNN_ERR_NOMEM 6        // device memory exhausted
+#define GSKNN_ERR_TIMEOUT 7      // a bounded device-side wait gave up
+
+namespace gsknn {
+
+struct SimtGeom {
+  int kp;      // list length (power of two >= k, >= 32), 0 when k is unsupported
+  int bq, br;  // queries / candidates per CTA tile
+  int dk;      // dimension chunk
+  size_t smem;
+  int nthr;
+};
+
+template <typename T>
+struct SimtArgs {
+  const T *Apack;        // query panels [qtiles][nkc][DK][BQ]
+  const T *Bpack;        // candidate panels [rtiles][nkc][DK][BR]
+  const T *qn;           // packed query norms [qtiles*BQ]
+  const T *cn;           // packed candidate norms [rtiles*BR] (NaN past the end)
+  const uint32_t *cid;   // packed candidate ids [rtiles*BR]
+  const T *Din;          // incoming heap (for the initial threshold), may be null
+  int ldD;
+  int Q, k, nkc;
+  int ntiles_r, tiles_per_split;
+  T *partD;              // [S][Q][k] sorted ascending
+  uint32_t *partI;
+};
+
+template <typename T>
+struct FinalizeArgs {
+  const T *Din;          // incoming heap rows (may alias Dout), may be null
+  const int *Iin;
+  int ldD;
+  int Q, k, S;
+  const T *partD;
+  const uint32_t *partI;
+  T *Dout;
+  int *Iout;
+};
+
+template <typename T>
+cudaError_t launch_pack(const T *X, const T *X2, int d, long long nrows, const int *idx,
+                        int count, int BT, int DK, int nkc, T *P, T *norms, uint32_t *ids,
+                        int *status, cudaStream_t st);
+template <typename T>
+SimtGeom simt_geometry(int k);
+template <typename T>
+cudaError_t launch_simt(const SimtArgs<T> &a, int kp, int qtiles, int S, cudaStream_t st);
+template <typename T>
+cudaError_t launch_finalize(const FinalizeArgs<T> &a, int kp, cudaStream_t st);
+
+}  // namespace gsknn
