@@ -50,6 +50,10 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target duration of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--queries", type=int, default=N_Q,
+                    help="query count of the device arm (smaller values are for profiling)")
+    ap.add_argument("--profile-only", action="store_true",
+                    help="device arm only: no end-to-end pass, no CPU baseline, no clocks")
     ap.add_argument("--cpu-worker", default=None, help=argparse.SUPPRESS)
     return ap.parse_args()
 
@@ -184,22 +188,23 @@ def run_ours(args, rank, world, local_rank):
     L = G.lib()
     # each rank its own query set (weak scaling); same reference set
     p = W.config2(seed=2)
+    nq = args.queries
     if world > 1:
-        beta_h = W.permutation(1000 + rank, N_POINTS)[:N_Q].astype(np.int32)
+        beta_h = W.permutation(1000 + rank, N_POINTS)[:nq].astype(np.int32)
     else:
-        beta_h = p.beta
+        beta_h = np.ascontiguousarray(p.beta[:nq])
     X = torch.from_numpy(p.X).to(dev)
     X2 = torch.from_numpy(p.X2).to(dev)
     alpha = torch.from_numpy(p.alpha).to(dev)
     beta = torch.from_numpy(beta_h).to(dev)
-    D = torch.empty((N_Q, K_NN), dtype=torch.float32, device=dev)
-    I = torch.empty((N_Q, K_NN), dtype=torch.int32, device=dev)
+    D = torch.empty((nq, K_NN), dtype=torch.float32, device=dev)
+    I = torch.empty((nq, K_NN), dtype=torch.int32, device=dev)
     st = torch.cuda.current_stream(dev)
 
     def step():
         D.fill_(float("inf"))
         I.fill_(-1)
-        rc = L.gsknn_s_device(N_R, N_Q, D_DIM, K_NN, X.data_ptr(), X2.data_ptr(), N_POINTS,
+        rc = L.gsknn_s_device(N_R, nq, D_DIM, K_NN, X.data_ptr(), X2.data_ptr(), N_POINTS,
                               alpha.data_ptr(), X.data_ptr(), X2.data_ptr(), N_POINTS,
                               beta.data_ptr(), D.data_ptr(), I.data_ptr(), K_NN, st.cuda_stream)
         if rc != 0:
@@ -217,8 +222,9 @@ def run_ours(args, rank, world, local_rank):
         raise RuntimeError(G.last_error())
 
     clocks = ClockSampler(local_rank)
-    clocks.start()
-    time.sleep(0.3)
+    if not args.profile_only:
+        clocks.start()
+        time.sleep(0.3)
     barrier()
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -244,11 +250,14 @@ def run_ours(args, rank, world, local_rank):
     kern = trace.get("fused_knn_simt")
     kern_ms = kern["ms"] / kern["launches"] if kern else None
 
+    evals = float(nq) * N_R
+    value = evals * world / (ms * 1e-3)
+    if args.profile_only:
+        return {"metric": "distance-evals/s", "value": value, "ms_per_step": ms,
+                "queries": nq, "kernels": trace, "profile_only": True}
+
     # end to end through the C ABI with host buffers (sgsknn_var1)
     e2e = e2e_host(L, p, beta_h, args, G)
-
-    evals = float(N_Q) * N_R
-    value = evals * world / (ms * 1e-3)
     out = {
         "metric": "distance-evals/s", "value": value, "unit": "distance-evals/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -352,7 +361,7 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     out = run_ours(args, rank, world, local_rank)
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.profile_only:
         try:
             out["cpu_baseline"] = cpu_baseline(args.cpu_seconds, threads)
         except Exception as e:  # reported, not fatal
