@@ -171,6 +171,35 @@ int gsknn_d_device(int m, int n, int d, int k, const double *XA, const double *X
 /* Synchronises `stream` and returns the device-side status of the last call enqueued on it. */
 int gsknn_stream_status(void *stream);
 
+/* gsknn_s_device without any memory allocation. No counterpart in the reference.
+ *
+ * For callers that must not allocate GPU memory while they run: a host program that hands all
+ * of the GPU's memory to its own fixed arena or caching pool up front (a surprise cudaMalloc then
+ * fails or evicts its cache), a latency-bound serving loop that cannot absorb cudaMalloc's cost
+ * or cudaFree's implicit device synchronisation in the middle of a request, and plugin hosts
+ * that forbid plugins from allocating device memory. Everything gsknn_s_device keeps in its
+ * per-stream cache
+ * here lives in one fixed 64 MiB array compiled into the library (each GPU that loads the
+ * library holds it until the process exits). The call itself allocates nothing; inputs and
+ * outputs are the caller's device buffers, with the same meaning as for gsknn_s_device.
+ *
+ * Limits and rules:
+ *   - the packed problem must fit the fixed scratch: about (m + n) * round_up(d, 16) * 4 bytes
+ *     of panels plus n * k * 8 bytes of partial lists; larger problems are rejected with
+ *     GSKNN_ERR_UNSUPPORTED and a message (nothing is launched), use gsknn_s_device for them;
+ *   - the first call on a device looks up the array's device address (cudaGetSymbolAddress)
+ *     with that device current; make that first call before any stream capture;
+ *   - every call on a device shares the one array and it keeps the last call's contents:
+ *     calls whose work may overlap on the GPU (different streams without ordering) race and
+ *     corrupt each other's results; serialise them, e.g. on one stream;
+ *   - `status` (device pointer, may be NULL) is cleared and then receives GSKNN_ERR_INDEX if
+ *     an alpha/beta entry lies outside its table; with NULL the check still guards the reads.
+ * Returns 0 when the work was enqueued on `stream`. */
+int gsknn_s_device_noalloc(int m, int n, int d, int k, const float *XA, const float *XA2,
+                           long long nA, const int *alpha, const float *XB, const float *XB2,
+                           long long nB, const int *beta, float *D, int *I, int ldD, int *status,
+                           void *stream);
+
 /* Launch tracing: while enabled, every kernel the library launches is bracketed by CUDA events
  * on its stream. gsknn_trace_read() waits for the recorded launches, writes a JSON object
  * {"kernel": {"launches": n, "ms": total}, ...} into buf and clears the record; it returns the
