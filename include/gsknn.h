@@ -151,8 +151,19 @@ const char *gsknn_last_error_string(void);
 #define GSKNN_MODE_FP32 1
 #define GSKNN_MODE_TF32 2
 #define GSKNN_MODE_BF16 3
+#define GSKNN_MODE_BF16X3 4 /* split BF16: hi*hi + hi*lo + lo*hi, near-FP32 distances */
 int gsknn_set_mode(int mode);
 int gsknn_get_mode(void);
+
+/* The tensor-core form on device pointers (roles and heaps as gsknn_s_device) in a given mode,
+ * which additionally writes the approximate distance of every (query j, candidate i) pair to
+ * C[j*ldc + i] (when C is not NULL) and each query's re-rank band 2E to margin[j] (when not
+ * NULL): every approximate distance lies within E of the exact FP64 distance. For tests and
+ * for callers that want the low-precision distance block itself. */
+int gsknn_tc_distances(int mode, int m, int n, int d, int k, const float *XA, const float *XA2,
+                       long long nA, const int *alpha, const float *XB, const float *XB2,
+                       long long nB, const int *beta, float *D, int *I, int ldD, float *C,
+                       long long ldc, float *margin, void *stream);
 
 /* Device-pointer entry points, asynchronous on `stream` (a cudaStream_t; NULL = the legacy
  * default stream). Roles as in dgsknn: m candidates alpha[] of table XA (nA rows), n queries
@@ -171,7 +182,8 @@ int gsknn_d_device(int m, int n, int d, int k, const double *XA, const double *X
 /* Synchronises `stream` and returns the device-side status of the last call enqueued on it. */
 int gsknn_stream_status(void *stream);
 
-/* gsknn_s_device without any memory allocation. No counterpart in the reference.
+/* gsknn_s_device in GSKNN_MODE_FP32 (the CUDA-core FP32 pipeline) without any memory
+ * allocation. No counterpart in the reference.
  *
  * For callers that must not allocate GPU memory while they run: a host program that hands all
  * of the GPU's memory to its own fixed arena or caching pool up front (a surprise cudaMalloc then

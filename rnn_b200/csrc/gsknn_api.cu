@@ -17,6 +17,7 @@
 #include <mutex>
 #include <string>
 #include <tuple>
+#include <type_traits>
 #include <vector>
 
 namespace gsknn {
@@ -181,13 +182,35 @@ static int choose_splits(int qtiles, int rtiles, int slots) {
   return best_s;
 }
 
+// Tracer hook for pipelines that bracket groups of launches themselves (the tensor-core path).
+static void trace_hook(void *, const char *name, bool begin, cudaStream_t st) {
+  if (!g_trace) return;
+  std::lock_guard<std::mutex> lk(g_tmu);
+  static thread_local std::vector<std::pair<const char *, cudaEvent_t>> pending;
+  if (begin) {
+    cudaEvent_t a = ev_get();
+    cudaEventRecord(a, st);
+    pending.push_back({name, a});
+    return;
+  }
+  for (size_t i = pending.size(); i-- > 0;) {
+    if (std::strcmp(pending[i].first, name) == 0) {
+      cudaEvent_t b = ev_get();
+      cudaEventRecord(b, st);
+      g_recs.push_back({name, pending[i].second, b});
+      pending.erase(pending.begin() + (long)i);
+      return;
+    }
+  }
+}
+
 // ------------------------------------------------------------------------------------------
 // device pipeline: pack -> fused select -> finalize (queries = heap rows)
 // ------------------------------------------------------------------------------------------
 template <typename T>
-int knn_device(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, long long nrows_q,
-               const int *qidx, const T *Xc, const T *Xc2, long long nrows_c, const int *cidx,
-               T *D, int *I, int ldD, cudaStream_t st) {
+int knn_device_simt(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, long long nrows_q,
+                    const int *qidx, const T *Xc, const T *Xc2, long long nrows_c,
+                    const int *cidx, T *D, int *I, int ldD, cudaStream_t st) {
   if (nq == 0 || nc == 0 || d == 0 || k == 0)
     return set_status(GSKNN_EARLY_RETURN, "early return: m, n, d or k is 0");
   if (nq < 0 || nc < 0 || d < 0 || k < 0 || ldD < k)
@@ -255,6 +278,65 @@ int knn_device(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, long lon
     CU(launch_finalize<T>(fa, g.kp, st));
   }
   return set_status(GSKNN_OK, nullptr);
+}
+
+static int g_mode = GSKNN_MODE_AUTO;
+
+// Tensor-core approximate pass + FP64 re-rank (float inputs). `dbg`, when set, also receives
+// the approximate distance of every (query, candidate) pair (row stride dbg_ld) and `margin`
+// the per-query band width 2E.
+static int knn_device_tc(int mode, int nq, int nc, int d, int k, const float *Xq,
+                         const float *Xq2, long long nrows_q, const int *qidx, const float *Xc,
+                         const float *Xc2, long long nrows_c, const int *cidx, float *D, int *I,
+                         int ldD, cudaStream_t st, float *dbg = nullptr, long long dbg_ld = 0,
+                         float *margin = nullptr) {
+  if (nq == 0 || nc == 0 || d == 0 || k == 0)
+    return set_status(GSKNN_EARLY_RETURN, "early return: m, n, d or k is 0");
+  if (nq < 0 || nc < 0 || d < 0 || k < 0 || ldD < k)
+    return set_status(GSKNN_ERR_ARG, "invalid sizes (n=%d m=%d d=%d k=%d ldD=%d)", nq, nc, d,
+                      k, ldD);
+  if (!Xq || !Xq2 || !qidx || !Xc || !Xc2 || !cidx || !D || !I)
+    return set_status(GSKNN_ERR_ARG, "null pointer argument");
+  const TcPlan P = tc_plan(nq, nc, d, k, mode, sm_count());
+  if (!P.ok)
+    return set_status(GSKNN_ERR_UNSUPPORTED,
+                      "tensor-core mode %d does not support d=%d k=%d (shared memory)", mode, d,
+                      k);
+  void *ws = nullptr, *stv = nullptr;
+  CU(scratch(SLOT_KERNEL, P.bytes, st, &ws));
+  CU(scratch(SLOT_STATUS, 256, st, &stv));
+  int *status = static_cast<int *>(stv);
+  CU(cudaMemsetAsync(status, 0, sizeof(int), st));
+  CU(tc_run(P, nq, nc, d, k, Xq, Xq2, nrows_q, qidx, Xc, Xc2, nrows_c, cidx, D, I, ldD, ws,
+            status, dbg, dbg_ld, st, trace_hook, nullptr));
+  if (margin)
+    CU(cudaMemcpyAsync(margin, static_cast<char *>(ws) + P.o_margin, (size_t)nq * 4,
+                       cudaMemcpyDeviceToDevice, st));
+  return set_status(GSKNN_OK, nullptr);
+}
+
+// The arithmetic used for a float call: explicit modes are honoured; AUTO takes the
+// tensor-core form with the exact FP64 re-rank where it fits (split BF16 below d = 128, TF32
+// from there), else the CUDA-core FP32 kernel.
+static int pick_mode(int nq, int nc, int d, int k) {
+  if (g_mode != GSKNN_MODE_AUTO) return g_mode;
+  const int m = d < 128 ? GSKNN_TC_BF16X3 : GSKNN_TC_TF32;
+  if (tc_plan(nq, nc, d, k, m, sm_count()).ok) return m;
+  return GSKNN_MODE_FP32;
+}
+
+template <typename T>
+int knn_device(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, long long nrows_q,
+               const int *qidx, const T *Xc, const T *Xc2, long long nrows_c, const int *cidx,
+               T *D, int *I, int ldD, cudaStream_t st) {
+  if constexpr (std::is_same<T, float>::value) {
+    const int mode = pick_mode(nq, nc, d, k);
+    if (mode != GSKNN_MODE_FP32)
+      return knn_device_tc(mode, nq, nc, d, k, Xq, Xq2, nrows_q, qidx, Xc, Xc2, nrows_c, cidx,
+                           D, I, ldD, st);
+  }
+  return knn_device_simt<T>(nq, nc, d, k, Xq, Xq2, nrows_q, qidx, Xc, Xc2, nrows_c, cidx, D, I,
+                            ldD, st);
 }
 
 // Reads back the device status word of `st` (after synchronising it).
@@ -352,8 +434,6 @@ int knn_host(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, const int 
   return set_status(GSKNN_OK, nullptr);
 }
 
-static int g_mode = GSKNN_MODE_AUTO;
-
 }  // namespace gsknn
 
 using namespace gsknn;
@@ -367,7 +447,7 @@ int gsknn_last_error(void) { return t_status; }
 const char *gsknn_last_error_string(void) { return t_msg; }
 
 int gsknn_set_mode(int mode) {
-  if (mode < GSKNN_MODE_AUTO || mode > GSKNN_MODE_BF16)
+  if (mode < GSKNN_MODE_AUTO || mode > GSKNN_MODE_BF16X3)
     return set_status(GSKNN_ERR_ARG, "unknown mode %d", mode);
   g_mode = mode;
   return set_status(GSKNN_OK, nullptr);
@@ -389,6 +469,17 @@ int gsknn_d_device(int m, int n, int d, int k, const double *XA, const double *X
 }
 
 int gsknn_stream_status(void *stream) { return device_status((cudaStream_t)stream); }
+
+int gsknn_tc_distances(int mode, int m, int n, int d, int k, const float *XA, const float *XA2,
+                       long long nA, const int *alpha, const float *XB, const float *XB2,
+                       long long nB, const int *beta, float *D, int *I, int ldD, float *C,
+                       long long ldc, float *margin, void *stream) {
+  if (mode != GSKNN_MODE_TF32 && mode != GSKNN_MODE_BF16 && mode != GSKNN_MODE_BF16X3)
+    return set_status(GSKNN_ERR_ARG, "gsknn_tc_distances: mode must be a tensor-core mode");
+  if (C && ldc < m) return set_status(GSKNN_ERR_ARG, "gsknn_tc_distances: ldc < m");
+  return knn_device_tc(mode, n, m, d, k, XB, XB2, nB, beta, XA, XA2, nA, alpha, D, I, ldD,
+                       (cudaStream_t)stream, C, ldc, margin);
+}
 
 void gsknn_trace_enable(int on) {
   std::lock_guard<std::mutex> lk(g_tmu);

@@ -63,4 +63,31 @@ cudaError_t launch_simt(const SimtArgs<T> &a, int kp, int qtiles, int S, cudaStr
 template <typename T>
 cudaError_t launch_finalize(const FinalizeArgs<T> &a, int kp, cudaStream_t st);
 
+// ---- tensor-core (tcgen05) precision form, float inputs ------------------------------------
+// Arithmetic formats of the approximate pass (the public GSKNN_MODE_* values map onto them).
+#define GSKNN_TC_TF32 2
+#define GSKNN_TC_BF16 3
+#define GSKNN_TC_BF16X3 4
+
+// Kernel-launch bracket used by the library's tracer (begin/end around a group of launches).
+typedef void (*TraceHook)(void *ctx, const char *name, bool begin, cudaStream_t st);
+
+struct TcPlan {
+  bool ok;
+  int fmt, elem, d_pad, nkc, a_terms, b_terms, kp;
+  int N, NST, qtiles, rtiles, q_pad, r_pad, S, tiles_per_split, logcap;
+  unsigned smem;
+  float coefA, coefB;
+  size_t o_mu, o_mu2, o_stats, o_pa, o_pa_lo, o_pb, o_pb_lo, o_qn, o_qnrm, o_cn, o_cnrm,
+      o_cid, o_log, o_logcnt, o_kth, o_margin, o_fbl, o_fbc;
+  size_t bytes;
+};
+
+TcPlan tc_plan(int nq, int nc, int d, int k, int mode, int sms);
+cudaError_t tc_run(const TcPlan &P, int nq, int nc, int d, int k, const float *Xq,
+                   const float *Xq2, long long nrows_q, const int *qidx, const float *Xc,
+                   const float *Xc2, long long nrows_c, const int *cidx, float *D, int *I,
+                   int ldD, void *ws, int *status, float *dbg, long long dbg_ld,
+                   cudaStream_t st, TraceHook hook, void *hook_ctx);
+
 }  // namespace gsknn

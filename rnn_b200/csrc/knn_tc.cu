@@ -1,0 +1,928 @@
+// knn_tc.cu -- the precision form of the fused kNN: tensor-core (tcgen05) distances in TF32,
+// BF16 or split BF16 (hi*hi + hi*lo + lo*hi), with FP32 accumulation in TMEM, followed by an
+// FP64 re-rank of every candidate whose approximate distance lies within a rigorous rounding
+// bound of the query's k-th approximate distance. The result is the exact FP64 top-k (ties to
+// the lower id) of the caller's float inputs, merged into the caller's heaps.
+//
+// Kernels (one call):
+//   tc_center     shift vector mu = mean of a strided sample of candidate rows
+//   tc_pack       one warp per row: gather, centre, round to the MMA format into a row-major
+//                 [rows][d_pad] panel (TMA source), effective norm X2 - 2 mu.x + mu.mu (the
+//                 centred norm, built on the caller's norm) in FP64, centred norm bound, ids;
+//                 running maxima for the bound
+//   tc_knn        warp 0 TMA producer, warp 1 MMA issuer (TMEM owner), warps 2-5 epilogue with
+//                 one query row per thread: approximate d' = qn' + cn' - 2<q~,c~>, a per-query
+//                 max-heap of the k smallest d' in shared memory (threshold), and a per-query
+//                 log in HBM of every candidate with d' <= k-th + 2E
+//   tc_rerank     one warp per query: exact FP64 distances of the logged band, sorted merge with
+//                 the incoming heap row, descending write-back (a valid max-heap)
+//   tc_fallback   queries whose log overflowed: exact FP64 brute force over all candidates
+//
+// Error bound (per query q, all candidates c; u = unit roundoff of the MMA input format,
+// M = max |c~|, CN = max |cn'|, D = padded dimension):
+//   |d'(q,c) - d(q,c)| <= E_q = 1.25 * [ 2 (2u + u^2 + D 2^-23 (1+u)^2) |q~| M
+//                                         + 3 * 2^-24 (CN + |qn'| + 2 |q~| M) ]
+// For the split format the input term 2u + u^2 is replaced by 3.2 u^2 (u = 2^-8) and the
+// accumulation term counts 3D products.
+#include "knn_common.cuh"
+#include "knn_internal.h"
+#include "tc_ptx.cuh"
+
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+
+namespace gsknn {
+namespace tc {
+
+constexpr int TC_M = 128;            // queries per CTA (TMEM lanes)
+constexpr int CHUNK_BYTES = 128;     // K bytes per TMA box / swizzle atom row
+constexpr int A_CHUNK = TC_M * CHUNK_BYTES;  // 16 KB
+constexpr int NTHREADS = 192;        // producer, MMA, 4 epilogue warps
+constexpr uint32_t LOG_OVF = 1u << 30;
+
+// ------------------------------------------------------------------------------------------
+// shift vector
+// ------------------------------------------------------------------------------------------
+__global__ void tc_center(const float *__restrict__ X, int d, long long nrows,
+                          const int *__restrict__ idx, int count, int nsample,
+                          float *__restrict__ mu, double *__restrict__ mu2) {
+  // one thread per dimension; strided sample of the candidate list
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < d) {
+    double s = 0.0;
+    int used = 0;
+    for (int t = 0; t < nsample; t++) {
+      const long long i = (long long)t * count / nsample;
+      const long long row = idx[i];
+      if (row >= 0 && row < nrows) {
+        s += (double)X[row * d + p];
+        used++;
+      }
+    }
+    mu[p] = used ? (float)(s / used) : 0.0f;
+  }
+}
+
+__global__ void tc_mu2(const float *__restrict__ mu, int d, double *__restrict__ mu2) {
+  double s = 0.0;
+  for (int p = threadIdx.x; p < d; p += 32) s += (double)mu[p] * (double)mu[p];
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(FULL_MASK, s, o);
+  if (threadIdx.x == 0) *mu2 = s;
+}
+
+// ------------------------------------------------------------------------------------------
+// packing
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+// fmt: 0 = TF32 (4-byte panel), 1 = BF16, 2 = split BF16 (hi and lo panels)
+__global__ void __launch_bounds__(256) tc_pack(
+    int fmt, const float *__restrict__ X, const float *__restrict__ X2, int d, int d_pad,
+    long long nrows, const int *__restrict__ idx, int count, int rows_pad,
+    const float *__restrict__ mu, const double *__restrict__ mu2, int is_cand, void *panel,
+    void *panel_lo, float *__restrict__ enorm, float *__restrict__ cnrm,
+    uint32_t *__restrict__ ids, unsigned *__restrict__ stats, int *__restrict__ status) {
+  const int lane = threadIdx.x & 31;
+  const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (r >= rows_pad) return;
+  long long row = -1;
+  if (r < count) {
+    row = idx[r];
+    if (row < 0 || row >= nrows) {
+      if (lane == 0) atomicExch(status, GSKNN_ERR_INDEX);
+      row = -1;
+    }
+  }
+  double s2 = 0.0, smx = 0.0;
+  for (int p = lane; p < d_pad; p += 32) {
+    float y = 0.0f;
+    if (row >= 0 && p < d) {
+      const float x = X[row * d + p];
+      const float m = mu[p];
+      y = x - m;
+      smx += (double)m * (double)x;
+      s2 += (double)y * (double)y;
+    }
+    const size_t o = (size_t)r * d_pad + p;
+    if (fmt == 0) {
+      reinterpret_cast<uint32_t *>(panel)[o] = to_tf32(y);
+    } else if (fmt == 1) {
+      reinterpret_cast<__nv_bfloat16 *>(panel)[o] = __float2bfloat16_rn(y);
+    } else {
+      const __nv_bfloat16 hi = __float2bfloat16_rn(y);
+      const __nv_bfloat16 lo = __float2bfloat16_rn(y - __bfloat162float(hi));
+      reinterpret_cast<__nv_bfloat16 *>(panel)[o] = hi;
+      reinterpret_cast<__nv_bfloat16 *>(panel_lo)[o] = lo;
+    }
+  }
+  for (int o = 16; o; o >>= 1) {
+    s2 += __shfl_xor_sync(FULL_MASK, s2, o);
+    smx += __shfl_xor_sync(FULL_MASK, smx, o);
+  }
+  if (lane == 0) {
+    if (row >= 0) {
+      // |x - mu|^2 expressed through the caller's norm: X2 - 2 mu.x + mu.mu
+      const double en = (double)X2[row] - 2.0 * smx + *mu2;
+      const float enf = (float)en;
+      // centred norm of the stored (FP32-rounded) shift, rounded up
+      const float nrm = (float)(sqrt(s2) * (1.0 + 1e-6)) * (1.0f + 1e-6f);
+      enorm[r] = enf;
+      cnrm[r] = nrm;
+      if (ids) ids[r] = (uint32_t)row;
+      if (is_cand) {
+        atomicMax(&stats[0], __float_as_uint(nrm));
+        atomicMax(&stats[1], __float_as_uint(fabsf(enf) * (1.0f + 1e-6f)));
+      }
+    } else {
+      enorm[r] = Num<float>::nan();
+      cnrm[r] = 0.0f;
+      if (ids) ids[r] = NO_ID;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// the tensor-core kernel
+// ------------------------------------------------------------------------------------------
+struct TcParams {
+  int Q, k, nkc, ntiles_r, tiles_per_split, N, NST, logcap;
+  int a_terms, b_terms, fmt;
+  uint32_t idesc;
+  const float *cn;
+  const uint32_t *cid;
+  const float *qn;
+  const float *qnrm;
+  const unsigned *stats;
+  const float *Din;
+  int ldD;
+  float coefA, coefB;
+  uint2 *log;
+  int *logcnt;
+  float *kth;
+  float *margin;
+  int *status;
+  float *dbg;
+  long long dbg_ld;
+  long long dbg_ncols;
+};
+
+struct SmemLayout {
+  uint32_t a_off, b_off, heap_off, bar_off, tmem_off, total;
+};
+
+__host__ __device__ inline SmemLayout tc_smem_layout(int nkc, int a_terms, int b_terms, int N,
+                                                     int NST, int k) {
+  SmemLayout L;
+  uint32_t off = 0;
+  L.a_off = off;
+  off += (uint32_t)a_terms * nkc * A_CHUNK;
+  L.b_off = off;
+  off += (uint32_t)NST * b_terms * N * CHUNK_BYTES;
+  L.heap_off = off;
+  off += (uint32_t)k * TC_M * 4;
+  off = (off + 7) & ~7u;
+  L.bar_off = off;
+  off += (uint32_t)(2 * NST + 5) * 8;
+  L.tmem_off = off;
+  off += 16;
+  L.total = off + 1024;  // alignment slack
+  return L;
+}
+
+struct EpiState {
+  float qn, E2, thr0, root, thr, Tv;
+  int cnt;
+  int ovf;
+};
+
+__device__ __forceinline__ void refresh_threshold(EpiState &s) {
+  float t = s.root + s.E2;
+  s.thr = t < s.thr0 ? t : s.thr0;
+  // filter in the v = d' - qn' space with slack for the rounding of the subtraction
+  s.Tv = (s.thr - s.qn) + (fabsf(s.thr) + fabsf(s.qn)) * 2.4e-7f + 1e-30f;
+}
+
+// Replace the heap root by x (< root) and sift down; returns the new root. Heap of k floats,
+// element i of this thread's query at heap[i * TC_M + row] (bank-conflict free across a warp).
+__device__ __noinline__ float heap_replace_root(float *heap, int row, int k, float x) {
+  int s = 0;
+  while (true) {
+    int c = 2 * s + 1;
+    if (c >= k) break;
+    float cv = heap[c * TC_M + row];
+    if (c + 1 < k) {
+      const float c2 = heap[(c + 1) * TC_M + row];
+      if (c2 > cv) { cv = c2; c = c + 1; }
+    }
+    if (!(cv > x)) break;
+    heap[s * TC_M + row] = cv;
+    s = c;
+  }
+  heap[s * TC_M + row] = x;
+  return heap[row];
+}
+
+// Drops log entries above the current threshold; returns the new count.
+__device__ __noinline__ int log_compact(uint2 *lg, int cnt, float thr) {
+  int w = 0;
+  for (int e = 0; e < cnt; e++) {
+    const uint2 x = lg[e];
+    if (__uint_as_float(x.x) <= thr) lg[w++] = x;
+  }
+  return w;
+}
+
+__device__ __forceinline__ void epi_candidate(EpiState &s, float v, uint32_t id, uint2 *lg,
+                                              int logcap, float *heap, int row, int k) {
+  const float dp = v + s.qn;
+  if (!(dp <= s.thr)) return;
+  if (!s.ovf) {
+    if (s.cnt >= logcap) {
+      s.cnt = log_compact(lg, s.cnt, s.thr);
+      if (s.cnt >= logcap) s.ovf = 1;
+    }
+    if (!s.ovf) lg[s.cnt++] = make_uint2(__float_as_uint(dp), id);
+  }
+  if (dp < s.root) {
+    s.root = heap_replace_root(heap, row, k, dp);
+    refresh_threshold(s);
+  }
+}
+
+template <int FMT>
+__global__ void __launch_bounds__(NTHREADS, 1)
+    tc_knn(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tAlo,
+           const __grid_constant__ CUtensorMap tB, const __grid_constant__ CUtensorMap tBlo,
+           const TcParams p) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  const uint32_t raw = su32(smem_raw);
+  unsigned char *smem = smem_raw + ((1024u - (raw & 1023u)) & 1023u);
+  const SmemLayout L = tc_smem_layout(p.nkc, p.a_terms, p.b_terms, p.N, p.NST, p.k);
+  unsigned char *sA = smem + L.a_off;
+  unsigned char *sB = smem + L.b_off;
+  float *heap = reinterpret_cast<float *>(smem + L.heap_off);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L.bar_off);
+  uint64_t *full = bars;
+  uint64_t *empty = bars + p.NST;
+  uint64_t *tfull = bars + 2 * p.NST;
+  uint64_t *tempty = bars + 2 * p.NST + 2;
+  uint64_t *afull = bars + 2 * p.NST + 4;
+  uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(smem + L.tmem_off);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int qt = blockIdx.x, split = blockIdx.y;
+  const int t_begin = split * p.tiles_per_split;
+  int t_end = t_begin + p.tiles_per_split;
+  if (t_end > p.ntiles_r) t_end = p.ntiles_r;
+  const int ntile = t_end > t_begin ? t_end - t_begin : 0;
+  const int N = p.N;
+  const uint32_t b_stage_bytes = (uint32_t)p.b_terms * N * CHUNK_BYTES;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < p.NST; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], 4);
+    }
+    mbar_init(afull, 1);
+    mbar_fence_init();
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_holder, (uint32_t)(2 * N));
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_holder;
+  bool failed = false;
+
+  if (warp == 0) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0 && ntile > 0) {
+      prefetch_tmap(&tA);
+      prefetch_tmap(&tB);
+      const int celems = FMT == 0 ? 32 : 64;
+      mbar_expect_tx(afull, (uint32_t)(p.a_terms * p.nkc * A_CHUNK));
+      for (int kc = 0; kc < p.nkc; kc++) {
+        tma_load_2d(sA + kc * A_CHUNK, &tA, kc * celems, qt * TC_M, afull);
+        if (FMT == 2)
+          tma_load_2d(sA + (p.nkc + kc) * A_CHUNK, &tAlo, kc * celems, qt * TC_M, afull);
+      }
+      int it = 0;
+      for (int lt = 0; lt < ntile && !failed; lt++) {
+        const int tile = t_begin + lt;
+        for (int kc = 0; kc < p.nkc; kc++, it++) {
+          const int s = it % p.NST;
+          const uint32_t round = (uint32_t)(it / p.NST);
+          if (!mbar_wait(&empty[s], (round & 1u) ^ 1u)) { failed = true; break; }
+          mbar_expect_tx(&full[s], b_stage_bytes);
+          unsigned char *dst = sB + (uint32_t)s * b_stage_bytes;
+          tma_load_2d(dst, &tB, kc * celems, tile * N, &full[s]);
+          if (FMT == 2)
+            tma_load_2d(dst + N * CHUNK_BYTES, &tBlo, kc * celems, tile * N, &full[s]);
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0 && ntile > 0) {
+      if (!mbar_wait(afull, 0)) failed = true;
+      tc_fence_after();
+      const uint32_t a_base = su32(sA), b_base = su32(sB);
+      int it = 0;
+      for (int lt = 0; lt < ntile && !failed; lt++) {
+        const int b = lt & 1;
+        const uint32_t use = (uint32_t)(lt >> 1);
+        if (!mbar_wait(&tempty[b], (use & 1u) ^ 1u)) { failed = true; break; }
+        tc_fence_after();
+        const uint32_t tmem_d = tmem_base + (uint32_t)(b * N);
+        for (int kc = 0; kc < p.nkc; kc++, it++) {
+          const int s = it % p.NST;
+          const uint32_t round = (uint32_t)(it / p.NST);
+          if (!mbar_wait(&full[s], round & 1u)) { failed = true; break; }
+          tc_fence_after();
+          const uint32_t a_chunk = a_base + (uint32_t)kc * A_CHUNK;
+          const uint32_t b_chunk = b_base + (uint32_t)s * b_stage_bytes;
+#pragma unroll
+          for (int ks = 0; ks < 4; ks++) {
+            const uint32_t off = (uint32_t)ks * 32u;
+            const uint64_t ad = sdesc_k_sw128(a_chunk + off);
+            const uint64_t bd = sdesc_k_sw128(b_chunk + off);
+            const uint32_t first = (kc == 0 && ks == 0) ? 0u : 1u;
+            if (FMT == 0) {
+              mma_tf32(tmem_d, ad, bd, p.idesc, first);
+            } else {
+              mma_f16(tmem_d, ad, bd, p.idesc, first);
+              if (FMT == 2) {
+                const uint64_t alo = sdesc_k_sw128(a_chunk + (uint32_t)p.nkc * A_CHUNK + off);
+                const uint64_t blo = sdesc_k_sw128(b_chunk + (uint32_t)N * CHUNK_BYTES + off);
+                mma_f16(tmem_d, ad, blo, p.idesc, 1u);
+                mma_f16(tmem_d, alo, bd, p.idesc, 1u);
+              }
+            }
+          }
+          mma_commit(&empty[s]);
+        }
+        if (!failed) mma_commit(&tfull[b]);
+      }
+    }
+  } else {
+    // ---------------- epilogue: one query row per thread ----------------
+    const int lq = warp & 3;  // TMEM lane quarter this warp may access
+    const int row = lq * 32 + lane;
+    const int gq = qt * TC_M + row;
+    const bool valid = gq < p.Q;
+    for (int i = 0; i < p.k; i++) heap[i * TC_M + row] = Num<float>::inf();
+    EpiState s;
+    s.cnt = 0;
+    s.ovf = 0;
+    s.root = Num<float>::inf();
+    s.qn = 0.0f;
+    s.E2 = 0.0f;
+    s.thr0 = Num<float>::inf();
+    if (valid) {
+      s.qn = p.qn[gq];
+      const float M = __uint_as_float(p.stats[0]);
+      const float CN = __uint_as_float(p.stats[1]);
+      const float qa = p.qnrm[gq];
+      const float E = p.coefA * qa * M + p.coefB * (CN + fabsf(s.qn) + 2.0f * qa * M);
+      s.E2 = 2.0f * E;
+      if (p.Din) {
+        float mx = -Num<float>::inf();
+        const float *rowD = p.Din + (size_t)gq * p.ldD;
+        for (int j = 0; j < p.k; j++) mx = fmaxf(mx, rowD[j]);
+        if (mx > -Num<float>::inf()) s.thr0 = mx + s.E2;
+      }
+      refresh_threshold(s);
+      if (split == 0) p.margin[gq] = s.E2;
+    } else {
+      s.thr = -Num<float>::inf();
+      s.Tv = -Num<float>::inf();
+    }
+    uint2 *lg = p.log + ((size_t)split * p.Q + (valid ? gq : 0)) * p.logcap;
+    for (int lt = 0; lt < ntile && !failed; lt++) {
+      const int b = lt & 1;
+      const uint32_t use = (uint32_t)(lt >> 1);
+      if (!mbar_wait(&tfull[b], use & 1u)) { failed = true; break; }
+      tc_fence_after();
+      const uint32_t taddr = tmem_base + ((uint32_t)(lq * 32) << 16) + (uint32_t)(b * N);
+      const int tile = t_begin + lt;
+      const size_t cbase = (size_t)tile * N;
+      for (int c0 = 0; c0 < N; c0 += 32) {
+        uint32_t r[32];
+        __syncwarp();
+        tmem_ld32(taddr + (uint32_t)c0, r);
+        tmem_wait_ld();
+        float v[32];
+        float mn = Num<float>::inf();
+        const float4 *cn4 = reinterpret_cast<const float4 *>(p.cn + cbase + c0);
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          const float4 c4 = __ldg(cn4 + j);
+          v[4 * j + 0] = fmaf(__uint_as_float(r[4 * j + 0]), -2.0f, c4.x);
+          v[4 * j + 1] = fmaf(__uint_as_float(r[4 * j + 1]), -2.0f, c4.y);
+          v[4 * j + 2] = fmaf(__uint_as_float(r[4 * j + 2]), -2.0f, c4.z);
+          v[4 * j + 3] = fmaf(__uint_as_float(r[4 * j + 3]), -2.0f, c4.w);
+        }
+#pragma unroll
+        for (int i = 0; i < 32; i++) mn = fminf(mn, v[i]);
+        if (p.dbg && valid) {
+          for (int i = 0; i < 32; i++) {
+            const long long col = (long long)cbase + c0 + i;
+            if (col < p.dbg_ncols) p.dbg[(size_t)gq * p.dbg_ld + col] = v[i] + s.qn;
+          }
+        }
+        if (mn <= s.Tv) {
+#pragma unroll
+          for (int i = 0; i < 32; i++) {
+            if (v[i] <= s.Tv)
+              epi_candidate(s, v[i], p.cid[cbase + c0 + i], lg, p.logcap, heap, row, p.k);
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty[b]);
+    }
+    if (valid) {
+      p.kth[(size_t)split * p.Q + gq] = s.root;
+      p.logcnt[(size_t)split * p.Q + gq] = s.cnt | (s.ovf ? (int)LOG_OVF : 0);
+    }
+  }
+  if (failed) atomicExch(p.status, GSKNN_ERR_TIMEOUT);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1) tmem_dealloc(tmem_base, (uint32_t)(2 * N));
+}
+
+// ------------------------------------------------------------------------------------------
+// FP64 re-rank of the logged band
+// ------------------------------------------------------------------------------------------
+struct RerankParams {
+  int Q, k, S, logcap, d;
+  const uint2 *log;
+  const int *logcnt;
+  const float *kth;
+  const float *margin;
+  const float *Xq, *Xq2, *Xc, *Xc2;
+  const int *qidx;
+  float *D;
+  int *I;
+  int ldD;
+  int *fallback_list;
+  int *fallback_count;
+};
+
+// Exact squared distance of the oracle: (-2 <q,c> + |c|^2) + |q|^2 in FP64 from float inputs,
+// clamped at zero; the dot product is split across the warp.
+__device__ __forceinline__ double exact_dist_warp(const float *q, const float *c, int d,
+                                                  double cc, double qq, int lane) {
+  double acc = 0.0;
+  for (int pp = lane; pp < d; pp += 32) acc = fma((double)q[pp], (double)c[pp], acc);
+#pragma unroll
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(FULL_MASK, acc, o);
+  double v = fma(-2.0, acc, cc) + qq;
+  return v < 0.0 ? 0.0 : v;
+}
+
+template <int E>
+__device__ __forceinline__ void write_heap_row(float *D, int *I, int ldD, int q, int k,
+                                               const double (&ld)[E], const uint32_t (&li)[E],
+                                               int lane) {
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    const int t = e * 32 + lane;
+    if (t < k) {
+      D[(size_t)q * ldD + (k - 1 - t)] = (float)ld[e];
+      I[(size_t)q * ldD + (k - 1 - t)] = (int)li[e];
+    }
+  }
+}
+
+template <int E>
+__device__ __forceinline__ void load_heap_row(const float *D, const int *I, int ldD, int q, int k,
+                                              double (&ld)[E], uint32_t (&li)[E], int lane) {
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    const int t = e * 32 + lane;
+    if (t < k) {
+      ld[e] = (double)D[(size_t)q * ldD + t];
+      li[e] = (uint32_t)I[(size_t)q * ldD + t];
+    } else {
+      ld[e] = Num<double>::inf();
+      li[e] = NO_ID;
+    }
+  }
+  warp_sort<double, E>(ld, li, lane);
+}
+
+template <int E>
+__global__ void __launch_bounds__(256) tc_rerank(RerankParams p) {
+  const int lane = threadIdx.x & 31;
+  const int q = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (q >= p.Q) return;
+  // overflowed logs: the whole query goes to the brute-force pass
+  bool ovf = false;
+  float T = Num<float>::inf();
+  for (int s = 0; s < p.S; s++) {
+    ovf |= (p.logcnt[(size_t)s * p.Q + q] & (int)LOG_OVF) != 0;
+    T = fminf(T, p.kth[(size_t)s * p.Q + q]);
+  }
+  if (ovf) {
+    if (lane == 0) p.fallback_list[atomicAdd(p.fallback_count, 1)] = q;
+    return;
+  }
+  const float E2 = p.margin[q];
+  float thr = T + E2;
+  {
+    float mx = -Num<float>::inf();
+    for (int j = lane; j < p.k; j += 32) mx = fmaxf(mx, p.D[(size_t)q * p.ldD + j]);
+    for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(FULL_MASK, mx, o));
+    if (mx > -Num<float>::inf()) thr = fminf(thr, mx + E2);
+  }
+  double ld[E];
+  uint32_t li[E];
+  load_heap_row<E>(p.D, p.I, p.ldD, q, p.k, ld, li, lane);
+  const long long qrow = p.qidx[q];
+  const float *qv = p.Xq + qrow * p.d;
+  const double qq = (double)p.Xq2[qrow];
+  double bd = Num<double>::inf();
+  uint32_t bi = NO_ID;
+  int nb = 0;
+  for (int s = 0; s < p.S; s++) {
+    const int cnt = p.logcnt[(size_t)s * p.Q + q];
+    const uint2 *lg = p.log + ((size_t)s * p.Q + q) * p.logcap;
+    for (int base = 0; base < cnt; base += 32) {
+      const int e = base + lane;
+      uint2 ent = make_uint2(0u, NO_ID);
+      bool take = false;
+      if (e < cnt) {
+        ent = lg[e];
+        take = __uint_as_float(ent.x) <= thr;
+      }
+      unsigned m = __ballot_sync(FULL_MASK, take);
+      while (m) {
+        const int j = __ffs(m) - 1;
+        m &= m - 1;
+        const uint32_t cid = __shfl_sync(FULL_MASK, ent.y, j);
+        const float *cv = p.Xc + (long long)cid * p.d;
+        const double dist = exact_dist_warp(qv, cv, p.d, (double)p.Xc2[cid], qq, lane);
+        if (lane == nb) { bd = dist; bi = cid; }
+        if (++nb == 32) {
+          double b1[1] = {bd};
+          uint32_t i1[1] = {bi};
+          warp_sort<double, 1>(b1, i1, lane);
+          warp_merge_32<double, E>(ld, li, b1[0], i1[0], lane);
+          bd = Num<double>::inf();
+          bi = NO_ID;
+          nb = 0;
+        }
+      }
+    }
+  }
+  if (nb > 0) {
+    double b1[1] = {bd};
+    uint32_t i1[1] = {bi};
+    warp_sort<double, 1>(b1, i1, lane);
+    warp_merge_32<double, E>(ld, li, b1[0], i1[0], lane);
+  }
+  write_heap_row<E>(p.D, p.I, p.ldD, q, p.k, ld, li, lane);
+}
+
+// ------------------------------------------------------------------------------------------
+// exact brute force for queries whose log overflowed (rare; one CTA per query)
+// ------------------------------------------------------------------------------------------
+struct FallbackParams {
+  int k, d, nc;
+  const float *Xq, *Xq2, *Xc, *Xc2;
+  const int *qidx, *cidx;
+  long long nrows_c;
+  float *D;
+  int *I;
+  int ldD;
+  const int *list;
+  const int *count;
+};
+
+template <int E>
+__global__ void __launch_bounds__(256) tc_fallback(FallbackParams p) {
+  __shared__ double sd[8][32 * E];
+  __shared__ uint32_t si[8][32 * E];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n = *p.count;
+  for (int w = blockIdx.x; w < n; w += gridDim.x) {
+    const int q = p.list[w];
+    const long long qrow = p.qidx[q];
+    const float *qv = p.Xq + qrow * p.d;
+    const double qq = (double)p.Xq2[qrow];
+    double ld[E];
+    uint32_t li[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) { ld[e] = Num<double>::inf(); li[e] = NO_ID; }
+    double kth = Num<double>::inf();
+    // each warp scans a strided share of the candidates, one candidate per lane at a time
+    for (int base = warp * 32; base < p.nc; base += 256) {
+      const int c = base + lane;
+      double dist = Num<double>::inf();
+      uint32_t id = NO_ID;
+      if (c < p.nc) {
+        const long long row = p.cidx[c];
+        if (row >= 0 && row < p.nrows_c) {
+          const float *cv = p.Xc + row * p.d;
+          double acc = 0.0;
+          for (int pp = 0; pp < p.d; pp++) acc = fma((double)qv[pp], (double)cv[pp], acc);
+          dist = fma(-2.0, acc, (double)p.Xc2[row]) + qq;
+          if (dist < 0.0) dist = 0.0;
+          id = (uint32_t)row;
+        }
+      }
+      if (__any_sync(FULL_MASK, dist <= kth)) {
+        double b1[1] = {dist};
+        uint32_t i1[1] = {id};
+        warp_sort<double, 1>(b1, i1, lane);
+        warp_merge_32<double, E>(ld, li, b1[0], i1[0], lane);
+        double t = ld[0];
+#pragma unroll
+        for (int e = 0; e < E; e++)
+          if (e == (p.k - 1) / 32) t = ld[e];
+        kth = __shfl_sync(FULL_MASK, t, (p.k - 1) & 31);
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      sd[warp][e * 32 + lane] = ld[e];
+      si[warp][e * 32 + lane] = li[e];
+    }
+    __syncthreads();
+    if (warp == 0) {
+      double md[E];
+      uint32_t mi[E];
+      load_heap_row<E>(p.D, p.I, p.ldD, q, p.k, md, mi, lane);
+      for (int w2 = 0; w2 < 8; w2++) {
+        double bd[E];
+        uint32_t bi[E];
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+          bd[e] = sd[w2][e * 32 + lane];
+          bi[e] = si[w2][e * 32 + lane];
+        }
+        warp_merge_lists<double, E>(md, mi, bd, bi, lane);
+      }
+      write_heap_row<E>(p.D, p.I, p.ldD, q, p.k, md, mi, lane);
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------------------------
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void *ptr = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(ptr);
+  }
+  return fn;
+}
+
+// Row-major [rows][d_pad] panel of elem-byte elements; box = 128 bytes x box_rows rows, 128B
+// swizzle (the K-major layout tcgen05 descriptors expect).
+static cudaError_t make_panel_map(CUtensorMap *m, void *base, int elem, int d_pad, int rows,
+                                  int box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return cudaErrorNotSupported;
+  cuuint64_t gdim[2] = {(cuuint64_t)d_pad, (cuuint64_t)rows};
+  cuuint64_t gstride[1] = {(cuuint64_t)d_pad * elem};
+  cuuint32_t box[2] = {(cuuint32_t)(CHUNK_BYTES / elem), (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(m, elem == 4 ? CU_TENSOR_MAP_DATA_TYPE_UINT32 : CU_TENSOR_MAP_DATA_TYPE_UINT16,
+                  2, base, gdim, gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+}  // namespace tc
+
+static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+int tc_format_of_mode(int mode) {
+  return mode == GSKNN_TC_BF16 ? 1 : mode == GSKNN_TC_BF16X3 ? 2 : 0;
+}
+
+TcPlan tc_plan(int nq, int nc, int d, int k, int mode, int sms) {
+  using namespace tc;
+  TcPlan P{};
+  P.ok = false;
+  P.fmt = tc_format_of_mode(mode);
+  const int elem = P.fmt == 0 ? 4 : 2;
+  const int celems = CHUNK_BYTES / elem;
+  P.elem = elem;
+  P.d_pad = ((d + celems - 1) / celems) * celems;
+  P.nkc = P.d_pad / celems;
+  P.a_terms = P.b_terms = P.fmt == 2 ? 2 : 1;
+  P.kp = 32;
+  while (P.kp < k) P.kp <<= 1;
+  if (k > 256) return P;
+  // candidate tile width and pipeline depth that fit in shared memory
+  const uint32_t smem_max = 227 * 1024;
+  int best_N = 0, best_NST = 0;
+  const int Ns[2] = {256, 128};
+  for (int ni = 0; ni < 2 && !best_N; ni++) {
+    const int N = Ns[ni];
+    if (P.fmt == 0 && N == 256 && P.nkc > 4) continue;  // keep the TF32 A tile room
+    for (int NST = 6; NST >= 2; NST--) {
+      SmemLayout L = tc_smem_layout(P.nkc, P.a_terms, P.b_terms, N, NST, k);
+      if (L.total <= smem_max) { best_N = N; best_NST = NST; break; }
+    }
+  }
+  if (!best_N) return P;
+  P.N = best_N;
+  P.NST = best_NST;
+  P.smem = tc_smem_layout(P.nkc, P.a_terms, P.b_terms, P.N, P.NST, k).total;
+  P.qtiles = (nq + TC_M - 1) / TC_M;
+  P.rtiles = (nc + P.N - 1) / P.N;
+  P.q_pad = P.qtiles * TC_M;
+  P.r_pad = P.rtiles * P.N;
+  // splits: balance waves (one CTA per SM)
+  int best_s = 1;
+  double best = 1e300;
+  for (int s = 1; s <= std::min(P.rtiles, 16); s++) {
+    const long long items = (long long)P.qtiles * s;
+    const double cost = (double)((items + sms - 1) / sms) / s * (1.0 + 0.01 * s);
+    if (cost < best - 1e-12) { best = cost; best_s = s; }
+  }
+  P.S = best_s;
+  P.tiles_per_split = (P.rtiles + P.S - 1) / P.S;
+  P.logcap = std::max(4 * P.kp, 512);
+  // workspace
+  size_t off = 0;
+  auto take = [&](size_t b) { size_t o = off; off = al256(off + b); return o; };
+  P.o_mu = take((size_t)d * 4);
+  P.o_mu2 = take(8);
+  P.o_stats = take(16);
+  P.o_pa = take((size_t)P.q_pad * P.d_pad * elem);
+  P.o_pa_lo = P.fmt == 2 ? take((size_t)P.q_pad * P.d_pad * elem) : 0;
+  P.o_pb = take((size_t)P.r_pad * P.d_pad * elem);
+  P.o_pb_lo = P.fmt == 2 ? take((size_t)P.r_pad * P.d_pad * elem) : 0;
+  P.o_qn = take((size_t)P.q_pad * 4);
+  P.o_qnrm = take((size_t)P.q_pad * 4);
+  P.o_cn = take((size_t)P.r_pad * 4);
+  P.o_cnrm = take((size_t)P.r_pad * 4);
+  P.o_cid = take((size_t)P.r_pad * 4);
+  P.o_log = take((size_t)P.S * nq * P.logcap * 8);
+  P.o_logcnt = take((size_t)P.S * nq * 4);
+  P.o_kth = take((size_t)P.S * nq * 4);
+  P.o_margin = take((size_t)nq * 4);
+  P.o_fbl = take((size_t)nq * 4);
+  P.o_fbc = take(16);
+  P.bytes = off;
+  // error-bound coefficients
+  const double D = (double)P.d_pad;
+  double inp, accum;
+  if (P.fmt == 2) {
+    const double u = 1.0 / 256.0;
+    inp = 3.2 * u * u;
+    accum = 3.0 * D * std::ldexp(1.0, -23);
+  } else {
+    const double u = P.fmt == 0 ? std::ldexp(1.0, -11) : std::ldexp(1.0, -8);
+    inp = 2.0 * u + u * u;
+    accum = D * std::ldexp(1.0, -23) * (1 + u) * (1 + u);
+  }
+  P.coefA = (float)(1.25 * 2.0 * (inp + accum + std::ldexp(1.0, -22)));
+  P.coefB = (float)(1.25 * 3.0 * std::ldexp(1.0, -24) + 1e-12);
+  P.ok = true;
+  return P;
+}
+
+cudaError_t tc_run(const TcPlan &P, int nq, int nc, int d, int k, const float *Xq,
+                   const float *Xq2, long long nrows_q, const int *qidx, const float *Xc,
+                   const float *Xc2, long long nrows_c, const int *cidx, float *D, int *I,
+                   int ldD, void *ws, int *status, float *dbg, long long dbg_ld,
+                   cudaStream_t st, TraceHook hook, void *hook_ctx) {
+  using namespace tc;
+  char *base = static_cast<char *>(ws);
+  float *mu = reinterpret_cast<float *>(base + P.o_mu);
+  double *mu2 = reinterpret_cast<double *>(base + P.o_mu2);
+  unsigned *stats = reinterpret_cast<unsigned *>(base + P.o_stats);
+  void *pa = base + P.o_pa;
+  void *pa_lo = P.fmt == 2 ? base + P.o_pa_lo : nullptr;
+  void *pb = base + P.o_pb;
+  void *pb_lo = P.fmt == 2 ? base + P.o_pb_lo : nullptr;
+  float *qn = reinterpret_cast<float *>(base + P.o_qn);
+  float *qnrm = reinterpret_cast<float *>(base + P.o_qnrm);
+  float *cn = reinterpret_cast<float *>(base + P.o_cn);
+  float *cnrm = reinterpret_cast<float *>(base + P.o_cnrm);
+  uint32_t *cid = reinterpret_cast<uint32_t *>(base + P.o_cid);
+  int *fbc = reinterpret_cast<int *>(base + P.o_fbc);
+  cudaError_t e;
+  e = cudaMemsetAsync(stats, 0, 16, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(fbc, 0, 16, st);
+  if (e != cudaSuccess) return e;
+
+  auto mark = [&](const char *name, bool begin) {
+    if (hook) hook(hook_ctx, name, begin, st);
+  };
+  mark("tc_pack", true);
+  const int nsample = std::min(nc, 4096);
+  tc_center<<<(d + 127) / 128, 128, 0, st>>>(Xc, d, nrows_c, cidx, nc, nsample, mu, mu2);
+  tc_mu2<<<1, 32, 0, st>>>(mu, d, mu2);
+  tc_pack<<<(P.r_pad + 7) / 8, 256, 0, st>>>(P.fmt, Xc, Xc2, d, P.d_pad, nrows_c, cidx, nc,
+                                            P.r_pad, mu, mu2, 1, pb, pb_lo, cn, cnrm, cid,
+                                            stats, status);
+  tc_pack<<<(P.q_pad + 7) / 8, 256, 0, st>>>(P.fmt, Xq, Xq2, d, P.d_pad, nrows_q, qidx, nq,
+                                            P.q_pad, mu, mu2, 0, pa, pa_lo, qn, qnrm, nullptr,
+                                            stats, status);
+  e = cudaGetLastError();
+  mark("tc_pack", false);
+  if (e != cudaSuccess) return e;
+
+  CUtensorMap mA, mAlo, mB, mBlo;
+  e = make_panel_map(&mA, pa, P.elem, P.d_pad, P.q_pad, TC_M);
+  if (e == cudaSuccess) e = make_panel_map(&mB, pb, P.elem, P.d_pad, P.r_pad, P.N);
+  if (e != cudaSuccess) return e;
+  mAlo = mA;
+  mBlo = mB;
+  if (P.fmt == 2) {
+    e = make_panel_map(&mAlo, pa_lo, P.elem, P.d_pad, P.q_pad, TC_M);
+    if (e == cudaSuccess) e = make_panel_map(&mBlo, pb_lo, P.elem, P.d_pad, P.r_pad, P.N);
+    if (e != cudaSuccess) return e;
+  }
+  TcParams tp{};
+  tp.Q = nq; tp.k = k; tp.nkc = P.nkc; tp.ntiles_r = P.rtiles;
+  tp.tiles_per_split = P.tiles_per_split; tp.N = P.N; tp.NST = P.NST; tp.logcap = P.logcap;
+  tp.a_terms = P.a_terms; tp.b_terms = P.b_terms; tp.fmt = P.fmt;
+  tp.idesc = idesc_f32acc(P.fmt == 0 ? 2u : 1u, TC_M, P.N);
+  tp.cn = cn; tp.cid = cid; tp.qn = qn; tp.qnrm = qnrm; tp.stats = stats;
+  tp.Din = D; tp.ldD = ldD; tp.coefA = P.coefA; tp.coefB = P.coefB;
+  tp.log = reinterpret_cast<uint2 *>(base + P.o_log);
+  tp.logcnt = reinterpret_cast<int *>(base + P.o_logcnt);
+  tp.kth = reinterpret_cast<float *>(base + P.o_kth);
+  tp.margin = reinterpret_cast<float *>(base + P.o_margin);
+  tp.status = status;
+  tp.dbg = dbg;
+  tp.dbg_ld = dbg_ld;
+  tp.dbg_ncols = nc;
+  dim3 grid(P.qtiles, P.S);
+  mark("tc_knn", true);
+  if (P.fmt == 0) {
+    e = cudaFuncSetAttribute(tc_knn<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, P.smem);
+    if (e == cudaSuccess) tc_knn<0><<<grid, NTHREADS, P.smem, st>>>(mA, mAlo, mB, mBlo, tp);
+  } else if (P.fmt == 1) {
+    e = cudaFuncSetAttribute(tc_knn<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, P.smem);
+    if (e == cudaSuccess) tc_knn<1><<<grid, NTHREADS, P.smem, st>>>(mA, mAlo, mB, mBlo, tp);
+  } else {
+    e = cudaFuncSetAttribute(tc_knn<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, P.smem);
+    if (e == cudaSuccess) tc_knn<2><<<grid, NTHREADS, P.smem, st>>>(mA, mAlo, mB, mBlo, tp);
+  }
+  if (e == cudaSuccess) e = cudaGetLastError();
+  mark("tc_knn", false);
+  if (e != cudaSuccess) return e;
+
+  RerankParams rp{};
+  rp.Q = nq; rp.k = k; rp.S = P.S; rp.logcap = P.logcap; rp.d = d;
+  rp.log = tp.log; rp.logcnt = tp.logcnt; rp.kth = tp.kth; rp.margin = tp.margin;
+  rp.Xq = Xq; rp.Xq2 = Xq2; rp.Xc = Xc; rp.Xc2 = Xc2; rp.qidx = qidx;
+  rp.D = D; rp.I = I; rp.ldD = ldD;
+  rp.fallback_list = reinterpret_cast<int *>(base + P.o_fbl);
+  rp.fallback_count = fbc;
+  FallbackParams fp{};
+  fp.k = k; fp.d = d; fp.nc = nc; fp.Xq = Xq; fp.Xq2 = Xq2; fp.Xc = Xc; fp.Xc2 = Xc2;
+  fp.qidx = qidx; fp.cidx = cidx; fp.nrows_c = nrows_c; fp.D = D; fp.I = I; fp.ldD = ldD;
+  fp.list = rp.fallback_list; fp.count = fbc;
+  const int rb = (nq + 7) / 8;
+  mark("tc_rerank", true);
+  switch (P.kp) {
+    case 32: tc_rerank<1><<<rb, 256, 0, st>>>(rp); tc_fallback<1><<<148, 256, 0, st>>>(fp); break;
+    case 64: tc_rerank<2><<<rb, 256, 0, st>>>(rp); tc_fallback<2><<<148, 256, 0, st>>>(fp); break;
+    case 128: tc_rerank<4><<<rb, 256, 0, st>>>(rp); tc_fallback<4><<<148, 256, 0, st>>>(fp); break;
+    case 256: tc_rerank<8><<<rb, 256, 0, st>>>(rp); tc_fallback<8><<<148, 256, 0, st>>>(fp); break;
+    default: return cudaErrorInvalidValue;
+  }
+  e = cudaGetLastError();
+  mark("tc_rerank", false);
+  return e;
+}
+
+}  // namespace gsknn

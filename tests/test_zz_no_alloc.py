@@ -56,6 +56,17 @@ def _same(Da, Ia, Db, Ib):
 
 
 def test_noalloc_matches_caching_entry_point_two_calls():
+    # the no-alloc variant runs the CUDA-core FP32 pipeline: compare with gsknn_s_device in
+    # the same arithmetic
+    prev = G.get_mode()
+    G.set_mode(G.MODE_FP32)
+    try:
+        _compare_two_calls()
+    finally:
+        G.set_mode(prev)
+
+
+def _compare_two_calls():
     import torch
     L, f = _bind()
     dev = torch.device("cuda:0")
