@@ -8,13 +8,21 @@ references as disjoint seeded index subsets, k = 32, heaps reset to +inf each st
 seeded; the reference publishes no dataset for this path.
 
 `value`  : distance evaluations per second (queries x references / step time) with the point
-           table, norms and index lists resident in HBM, through the device entry point.
+           table, norms and index lists resident in HBM, through the device entry point, in
+           the library's default arithmetic (AUTO: tensor-core distances + FP64 re-rank, which
+           returns the exact FP64 neighbour sets).
 `e2e`    : the same metric through the reference-facing C ABI (sgsknn_var1) with host buffers:
            each step copies the referenced table rows, norms, index lists and heaps to the GPU
            and the heaps back.
-`roofline`: the fused selection kernel's achieved FP32 rate (2d+3 flops per evaluation, the
-           reference's count, test/test_dgsknn.c:243) against the CUDA-core FP32 peak at the
-           sampled SM clock (148 SMs x 128 lanes x 2 flops x clock).
+`modes`  : the same workload per arithmetic: plain FP32 CUDA-core kernel, TF32, BF16 and split
+           BF16 tensor-core forms.
+`precision_form`: the precision workload (32,768 queries x 262,144 references, d = 256, k = 64,
+           points on an 8-dim latent manifold + noise): TF32 / BF16 tensor-core + FP64 re-rank
+           against the plain FP32 kernel, with the tensor pipe's roofline.
+`roofline`: the dominant kernel of the headline run; contraction counted as 2d flops per
+           evaluation, against the measured bf16 dense peak (MEASURED_PEAKS.json; half of it
+           for TF32, the TF32 tensor rate) or, for the CUDA-core kernel, the FP32 issue rate at
+           the sampled SM clock.
 `cpu_baseline`: the reference's own sgsknn (compiled from its sources, oracle/_ref) on this
            host's cores, on a slice of the queries against all references.
 
@@ -36,9 +44,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 N_POINTS, D_DIM, N_Q, N_R, K_NN = 1 << 20, 64, 65536, 262144, 32
-FLOPS_PER_EVAL = 2 * D_DIM + 3
 WORKLOAD = (f"plain sgsknn float32: N={N_POINTS} d={D_DIM} gaussian-mixture(16, sigma=0.05), "
             f"queries={N_Q} references={N_R} k={K_NN}")
+MODE_NAMES = {0: "auto", 1: "fp32", 2: "tf32", 3: "bf16", 4: "bf16x3"}
+DOMINANT = {"fp32": "fused_knn_simt", "tf32": "tc_knn", "bf16": "tc_knn", "bf16x3": "tc_knn"}
 
 
 def parse():
@@ -52,10 +61,24 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--queries", type=int, default=N_Q,
                     help="query count of the device arm (smaller values are for profiling)")
+    ap.add_argument("--mode", default="auto", choices=list(MODE_NAMES.values()),
+                    help="arithmetic of the headline run")
     ap.add_argument("--profile-only", action="store_true",
-                    help="device arm only: no end-to-end pass, no CPU baseline, no clocks")
+                    help="headline device run only: no e2e, modes, precision form, CPU baseline")
+    ap.add_argument("--precision-only", action="store_true",
+                    help="only the precision-form workload (d=256), for profiling")
     ap.add_argument("--cpu-worker", default=None, help=argparse.SUPPRESS)
     return ap.parse_args()
+
+
+def load_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "bf16": d.get("bf16_tflops", 1590.0),
+                "bf16_sustained": d.get("bf16_tflops_sustained", 1400.0), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16": 1590.0, "bf16_sustained": 1400.0, "source": "fallback"}
 
 
 # ------------------------------------------------------------------------------------------
@@ -63,14 +86,13 @@ def parse():
 # ------------------------------------------------------------------------------------------
 def cpu_worker(spec: str) -> None:
     """Time the reference sgsknn (or the oracle port when the reference library is absent) on
-    `q_count` queries against all references. Prints one JSON line."""
+    a slice of the queries against all references. Prints one JSON line."""
     cfg = json.loads(spec)
     nthreads = cfg["threads"]
     os.environ["OMP_NUM_THREADS"] = str(nthreads)
     os.environ["GSKNN_IC_NT"] = str(nthreads)
     from rnn_b200 import workloads as W
     p = W.config2(seed=cfg["seed"])
-    import ctypes
     ref_so = os.path.join(ROOT, "oracle", "_ref", "libgsknn_ref.so")
     kind = "reference" if os.path.exists(ref_so) else "port"
     if kind == "reference":
@@ -177,112 +199,6 @@ class ClockSampler:
 # ------------------------------------------------------------------------------------------
 # the GPU arm
 # ------------------------------------------------------------------------------------------
-def run_ours(args, rank, world, local_rank):
-    import ctypes
-    import torch
-    from rnn_b200 import gsknn as G
-    from rnn_b200 import workloads as W
-
-    dev = torch.device("cuda", local_rank)
-    torch.cuda.set_device(dev)
-    L = G.lib()
-    # each rank its own query set (weak scaling); same reference set
-    p = W.config2(seed=2)
-    nq = args.queries
-    if world > 1:
-        beta_h = W.permutation(1000 + rank, N_POINTS)[:nq].astype(np.int32)
-    else:
-        beta_h = np.ascontiguousarray(p.beta[:nq])
-    X = torch.from_numpy(p.X).to(dev)
-    X2 = torch.from_numpy(p.X2).to(dev)
-    alpha = torch.from_numpy(p.alpha).to(dev)
-    beta = torch.from_numpy(beta_h).to(dev)
-    D = torch.empty((nq, K_NN), dtype=torch.float32, device=dev)
-    I = torch.empty((nq, K_NN), dtype=torch.int32, device=dev)
-    st = torch.cuda.current_stream(dev)
-
-    def step():
-        D.fill_(float("inf"))
-        I.fill_(-1)
-        rc = L.gsknn_s_device(N_R, nq, D_DIM, K_NN, X.data_ptr(), X2.data_ptr(), N_POINTS,
-                              alpha.data_ptr(), X.data_ptr(), X2.data_ptr(), N_POINTS,
-                              beta.data_ptr(), D.data_ptr(), I.data_ptr(), K_NN, st.cuda_stream)
-        if rc != 0:
-            raise RuntimeError(G.last_error())
-
-    def barrier():
-        if world > 1:
-            import torch.distributed as dist
-            dist.barrier()
-
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    if L.gsknn_stream_status(ctypes.c_void_p(st.cuda_stream)) != 0:
-        raise RuntimeError(G.last_error())
-
-    clocks = ClockSampler(local_rank)
-    if not args.profile_only:
-        clocks.start()
-        time.sleep(0.3)
-    barrier()
-    torch.cuda.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    # the library brackets each of its kernel launches with CUDA events on its stream
-    L.gsknn_trace_read(None, 0)
-    L.gsknn_trace_enable(1)
-    ev0.record(st)
-    for _ in range(args.steps):
-        step()
-    ev1.record(st)
-    torch.cuda.synchronize()
-    L.gsknn_trace_enable(0)
-    barrier()
-    ms = ev0.elapsed_time(ev1) / args.steps
-    clk = clocks.stop()
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    trace = read_trace(L)
-    launches = sum(v["launches"] for v in trace.values())
-    kern = trace.get("fused_knn_simt")
-    kern_ms = kern["ms"] / kern["launches"] if kern else None
-
-    evals = float(nq) * N_R
-    value = evals * world / (ms * 1e-3)
-    if args.profile_only:
-        return {"metric": "distance-evals/s", "value": value, "ms_per_step": ms,
-                "queries": nq, "kernels": trace, "profile_only": True}
-
-    # end to end through the C ABI with host buffers (sgsknn_var1)
-    e2e = e2e_host(L, p, beta_h, args, G)
-    out = {
-        "metric": "distance-evals/s", "value": value, "unit": "distance-evals/s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic (seeded gaussian mixture; no dataset published)",
-        "mode": "plain FP32 CUDA-core fused kernel",
-        "config": {"workload": WORKLOAD, "points": N_POINTS, "d": D_DIM, "queries": N_Q,
-                   "references": N_R, "k": K_NN, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (256 MiB point table gathered every step)"},
-        "gpu_launches": launches,
-        "kernels": trace,
-        "clocks": clk,
-    }
-    if kern_ms is not None:
-        sm_mhz = clk.get("sm_mhz") or 1965.0
-        peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
-        achieved = evals * FLOPS_PER_EVAL / (kern_ms * 1e-3) / 1e12
-        out["roofline"] = {"bound": "fp32-cuda-core", "achieved": achieved, "peak": peak,
-                           "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
-                           "kernel": "fused_knn_simt", "kernel_ms": kern_ms,
-                           "peak_source": "nominal FP32 issue rate at the sampled SM clock"}
-    out["e2e"] = e2e
-    return out
-
-
 def read_trace(L) -> dict:
     """Per-kernel launch counts and total milliseconds recorded by the library's tracer."""
     import ctypes
@@ -291,39 +207,242 @@ def read_trace(L) -> dict:
     return json.loads(buf.value.decode() or "{}")
 
 
-def e2e_host(L, p, beta_h, args, G):
+class DeviceProblem:
+    """A float kNN problem resident on the device, callable through gsknn_s_device."""
+
+    def __init__(self, p, beta_h, dev):
+        import torch
+        self.torch = torch
+        self.p = p
+        self.nq = beta_h.size
+        self.X = torch.from_numpy(p.X).to(dev)
+        self.X2 = torch.from_numpy(p.X2).to(dev)
+        self.alpha = torch.from_numpy(p.alpha).to(dev)
+        self.beta = torch.from_numpy(beta_h).to(dev)
+        self.D = torch.empty((self.nq, p.k), dtype=torch.float32, device=dev)
+        self.I = torch.empty((self.nq, p.k), dtype=torch.int32, device=dev)
+        self.st = torch.cuda.current_stream(dev)
+
+    @property
+    def evals(self):
+        return float(self.nq) * self.p.m
+
+    def step(self, L, G):
+        self.D.fill_(float("inf"))
+        self.I.fill_(-1)
+        n_rows = self.p.X.shape[0]
+        rc = L.gsknn_s_device(self.p.m, self.nq, self.p.d, self.p.k, self.X.data_ptr(),
+                              self.X2.data_ptr(), n_rows, self.alpha.data_ptr(),
+                              self.X.data_ptr(), self.X2.data_ptr(), n_rows,
+                              self.beta.data_ptr(), self.D.data_ptr(), self.I.data_ptr(),
+                              self.p.k, self.st.cuda_stream)
+        if rc != 0:
+            raise RuntimeError(G.last_error())
+
+
+def timed(L, G, prob, mode, steps, warmup, barrier=None, clocks=None):
+    """Warm-up, then `steps` calls bracketed by events on the launching stream with the
+    library's per-kernel tracer on. Returns (ms per step, trace)."""
+    import ctypes
+    torch = prob.torch
+    G.set_mode(mode)
+    for _ in range(warmup):
+        prob.step(L, G)
+    torch.cuda.synchronize()
+    if L.gsknn_stream_status(ctypes.c_void_p(prob.st.cuda_stream)) != 0:
+        raise RuntimeError(G.last_error())
+    if clocks:
+        clocks.start()
+        time.sleep(0.3)
+    if barrier:
+        barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    read_trace(L)
+    L.gsknn_trace_enable(1)
+    ev0.record(prob.st)
+    for _ in range(steps):
+        prob.step(L, G)
+    ev1.record(prob.st)
+    torch.cuda.synchronize()
+    L.gsknn_trace_enable(0)
+    if barrier:
+        barrier()
+    if L.gsknn_stream_status(ctypes.c_void_p(prob.st.cuda_stream)) != 0:
+        raise RuntimeError(G.last_error())
+    return ev0.elapsed_time(ev1) / steps, read_trace(L)
+
+
+def roofline(mode_name, prob, trace, peaks, clk):
+    kname = DOMINANT[mode_name]
+    kern = trace.get(kname)
+    if not kern:
+        return None
+    kms = kern["ms"] / kern["launches"]
+    d = prob.p.d
+    if mode_name == "fp32":
+        flops = prob.evals * (2 * d + 3)
+        sm_mhz = (clk or {}).get("sm_mhz") or 1965.0
+        peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+        src = "nominal FP32 CUDA-core issue rate at the sampled SM clock"
+        bound = "fp32"
+    else:
+        flops = prob.evals * 2 * d
+        peak = peaks["bf16"] * (0.5 if mode_name == "tf32" else 1.0)
+        src = (f"{peaks['source']} bf16 dense burst peak"
+               + (" x 0.5 (TF32 tensor rate)" if mode_name == "tf32" else ""))
+        bound = "tensor"
+    achieved = flops / (kms * 1e-3) / 1e12
+    out = {"bound": bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+           "frac": achieved / peak, "traffic": None, "kernel": kname, "kernel_ms": kms,
+           "peak_source": src}
+    if mode_name == "bf16x3":
+        out["executed_frac"] = 3 * achieved / peak
+        out["note"] = "split BF16 runs 3 MMAs per product; achieved counts the 2d useful flops"
+    return out
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from rnn_b200 import gsknn as G
+    from rnn_b200 import workloads as W
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    L = G.lib()
+    peaks = load_peaks()
+    name2mode = {v: k for k, v in MODE_NAMES.items()}
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    out = {}
+    if not args.precision_only:
+        p = W.config2(seed=2)
+        nq = args.queries
+        if world > 1:
+            beta_h = W.permutation(1000 + rank, N_POINTS)[:nq].astype(np.int32)
+        else:
+            beta_h = np.ascontiguousarray(p.beta[:nq])
+        prob = DeviceProblem(p, beta_h, dev)
+        clocks = ClockSampler(local_rank) if not args.profile_only else None
+        mode = name2mode[args.mode]
+        ms, trace = timed(L, G, prob, mode, args.steps, args.warmup, barrier, clocks)
+        clk = clocks.stop() if clocks else None
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        used = effective_mode_name(trace, p.d)
+        value = prob.evals * world / (ms * 1e-3)
+        out = {
+            "metric": "distance-evals/s", "value": value, "unit": "distance-evals/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 inputs; " + {"fp32": "fp32 CUDA-core distances",
+                                       "tf32": "tf32 tensor distances + fp64 re-rank",
+                                       "bf16": "bf16 tensor distances + fp64 re-rank",
+                                       "bf16x3": "split-bf16 tensor distances + fp64 re-rank"}[used],
+            "data": "synthetic (seeded gaussian mixture; no dataset published)",
+            "mode": f"{args.mode} -> {used}",
+            "exact_recall": used != "fp32",
+            "config": {"workload": WORKLOAD, "points": N_POINTS, "d": D_DIM, "queries": nq,
+                       "references": N_R, "k": K_NN, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (256 MiB point table gathered every step)"},
+            "gpu_launches": sum(v["launches"] for v in trace.values()),
+            "kernels": trace,
+            "clocks": clk,
+            "roofline": roofline(used, prob, trace, peaks, clk),
+        }
+        if args.profile_only:
+            return out
+        out["e2e"] = e2e_host(L, G, p, beta_h, args)
+        if world == 1:
+            modes = {}
+            for nm in ("fp32", "tf32", "bf16", "bf16x3"):
+                steps = 2 if nm == "fp32" else 5
+                mms, tr = timed(L, G, prob, name2mode[nm], steps, 1)
+                modes[nm] = {"ms_per_step": mms, "value": prob.evals / (mms * 1e-3),
+                             "roofline": roofline(nm, prob, tr, peaks, clk)}
+            out["modes"] = modes
+        del prob
+        torch.cuda.empty_cache()
+    if world == 1:
+        pf = precision_form(L, G, W, dev, peaks, args)
+        if args.precision_only:
+            return pf
+        out["precision_form"] = pf
+    G.set_mode(0)
+    return out
+
+
+def effective_mode_name(trace, d):
+    if "tc_knn" not in trace:
+        return "fp32"
+    from rnn_b200 import gsknn as G
+    m = G.get_mode()
+    if m == 0:
+        return "bf16x3" if d < 128 else "tf32"
+    return MODE_NAMES[m]
+
+
+def precision_form(L, G, W, dev, peaks, args):
+    """32,768 queries x 262,144 references, d = 256, k = 64, latent-manifold points."""
+    import torch
+    p = W.config3(seed=3)
+    prob = DeviceProblem(p, p.beta, dev)
+    res = {"workload": "precision form: queries=32768 references=262144 d=256 k=64, "
+                       "U[0,1)^8 latent through a seeded orthonormal basis + N(0,1e-3^2)"}
+    name2mode = {v: k for k, v in MODE_NAMES.items()}
+    for nm, steps in (("fp32", 2), ("tf32", 5), ("bf16", 5), ("bf16x3", 5)):
+        ms, tr = timed(L, G, prob, name2mode[nm], steps, 1)
+        res[nm] = {"ms_per_step": ms, "value": prob.evals / (ms * 1e-3),
+                   "roofline": roofline(nm, prob, tr, peaks, None), "kernels": tr}
+    base = res["fp32"]["value"]
+    for nm in ("tf32", "bf16", "bf16x3"):
+        res[nm]["speedup_vs_plain_fp32"] = res[nm]["value"] / base
+    del prob
+    torch.cuda.empty_cache()
+    return res
+
+
+def e2e_host(L, G, p, beta_h, args):
     import ctypes
     import torch
-    Xh, X2h = p.X, p.X2
-    alpha_h = p.alpha
-    D = np.empty((N_Q, K_NN), dtype=np.float32)
-    I = np.empty((N_Q, K_NN), dtype=np.int32)
+    nq = beta_h.size
+    D = np.empty((nq, K_NN), dtype=np.float32)
+    I = np.empty((nq, K_NN), dtype=np.int32)
     c_i = ctypes.c_int
+    G.set_mode(0)
 
     def call():
         D.fill(np.inf)
         I.fill(-1)
-        L.sgsknn_var1(c_i(N_Q), c_i(N_R), c_i(D_DIM), c_i(K_NN), G._p(Xh), G._p(X2h),
-                      G._p(beta_h), G._p(Xh), G._p(X2h), G._p(alpha_h), G._p(D), G._p(I))
+        L.sgsknn_var1(c_i(nq), c_i(N_R), c_i(D_DIM), c_i(K_NN), G._p(p.X), G._p(p.X2),
+                      G._p(beta_h), G._p(p.X), G._p(p.X2), G._p(p.alpha), G._p(D), G._p(I))
         code, msg = G.last_error()
         if code != 0:
             raise RuntimeError(msg)
 
     call()
-    steps = max(2, min(args.steps, 5))
+    steps = max(3, min(args.steps, 5))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(steps):
         call()
     t = (time.perf_counter() - t0) / steps
-    lo = int(min(beta_h.min(), alpha_h.min()))
-    hi = int(max(beta_h.max(), alpha_h.max()))
+    lo = int(min(beta_h.min(), p.alpha.min()))
+    hi = int(max(beta_h.max(), p.alpha.max()))
     rows = hi - lo + 1
-    h2d = rows * D_DIM * 4 + rows * 4 + (N_Q + N_R) * 4 + 2 * N_Q * K_NN * 4
-    d2h = 2 * N_Q * K_NN * 4
-    return {"value": float(N_Q) * N_R / t, "unit": "distance-evals/s", "ms_per_step": t * 1e3,
+    h2d = rows * D_DIM * 4 + rows * 4 + (nq + N_R) * 4 + 2 * nq * K_NN * 4
+    d2h = 2 * nq * K_NN * 4
+    return {"value": float(nq) * N_R / t, "unit": "distance-evals/s", "ms_per_step": t * 1e3,
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-            "api": "sgsknn_var1 (host pointers, pageable numpy buffers)"}
+            "api": "sgsknn_var1 (host pointers, pageable numpy buffers), default mode"}
 
 
 def main():
@@ -361,7 +480,8 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     out = run_ours(args, rank, world, local_rank)
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.profile_only:
+    if (rank == 0 and world == 1 and not args.no_cpu_baseline and not args.profile_only
+            and not args.precision_only):
         try:
             out["cpu_baseline"] = cpu_baseline(args.cpu_seconds, threads)
         except Exception as e:  # reported, not fatal

@@ -45,23 +45,37 @@ constexpr uint32_t LOG_OVF = 1u << 30;
 // ------------------------------------------------------------------------------------------
 // shift vector
 // ------------------------------------------------------------------------------------------
-__global__ void tc_center(const float *__restrict__ X, int d, long long nrows,
-                          const int *__restrict__ idx, int count, int nsample,
-                          float *__restrict__ mu, double *__restrict__ mu2) {
-  // one thread per dimension; strided sample of the candidate list
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p < d) {
-    double s = 0.0;
-    int used = 0;
-    for (int t = 0; t < nsample; t++) {
-      const long long i = (long long)t * count / nsample;
-      const long long row = idx[i];
-      if (row >= 0 && row < nrows) {
-        s += (double)X[row * d + p];
-        used++;
-      }
+// Block of 32 warps per 32 dimensions: lane = dimension, warps stride over a strided sample of
+// the candidate rows (coalesced 128-byte row segments), then a block reduction.
+__global__ void __launch_bounds__(1024) tc_center(const float *__restrict__ X, int d,
+                                                  long long nrows, const int *__restrict__ idx,
+                                                  int count, int nsample,
+                                                  float *__restrict__ mu) {
+  __shared__ double ps[32][33];
+  __shared__ int pc[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int p = blockIdx.x * 32 + lane;
+  double s = 0.0;
+  int used = 0;
+  for (int t = warp; t < nsample; t += 32) {
+    const long long i = (long long)t * count / nsample;
+    const long long row = idx[i];
+    if (row >= 0 && row < nrows) {
+      if (p < d) s += (double)X[row * d + p];
+      used++;
     }
-    mu[p] = used ? (float)(s / used) : 0.0f;
+  }
+  ps[warp][lane] = s;
+  if (lane == 0) pc[warp] = used;
+  __syncthreads();
+  if (warp == 0) {
+    double tot = 0.0;
+    int n = 0;
+    for (int w = 0; w < 32; w++) {
+      tot += ps[w][lane];
+      n += pc[w];
+    }
+    if (p < d) mu[p] = n ? (float)(tot / n) : 0.0f;
   }
 }
 
@@ -173,7 +187,7 @@ struct TcParams {
 };
 
 struct SmemLayout {
-  uint32_t a_off, b_off, heap_off, bar_off, tmem_off, total;
+  uint32_t a_off, b_off, heap_off, cn_off, bar_off, tmem_off, total;
 };
 
 __host__ __device__ inline SmemLayout tc_smem_layout(int nkc, int a_terms, int b_terms, int N,
@@ -186,9 +200,12 @@ __host__ __device__ inline SmemLayout tc_smem_layout(int nkc, int a_terms, int b
   off += (uint32_t)NST * b_terms * N * CHUNK_BYTES;
   L.heap_off = off;
   off += (uint32_t)k * TC_M * 4;
+  off = (off + 15) & ~15u;
+  L.cn_off = off;  // candidate norms of the two tiles in TMEM, copied by the MMA warp
+  off += 2u * N * 4;
   off = (off + 7) & ~7u;
   L.bar_off = off;
-  off += (uint32_t)(2 * NST + 5) * 8;
+  off += (uint32_t)(2 * NST + 7) * 8;
   L.tmem_off = off;
   off += 16;
   L.total = off + 1024;  // alignment slack
@@ -210,7 +227,7 @@ __device__ __forceinline__ void refresh_threshold(EpiState &s) {
 
 // Replace the heap root by x (< root) and sift down; returns the new root. Heap of k floats,
 // element i of this thread's query at heap[i * TC_M + row] (bank-conflict free across a warp).
-__device__ __noinline__ float heap_replace_root(float *heap, int row, int k, float x) {
+__device__ __forceinline__ float heap_replace_root(float *heap, int row, int k, float x) {
   int s = 0;
   while (true) {
     int c = 2 * s + 1;
@@ -228,12 +245,17 @@ __device__ __noinline__ float heap_replace_root(float *heap, int row, int k, flo
   return heap[row];
 }
 
-// Drops log entries above the current threshold; returns the new count.
+// Drops log entries above the current threshold; returns the new count. Reads in batches of
+// 16 before writing (writes never pass the read position), so the loads overlap.
 __device__ __noinline__ int log_compact(uint2 *lg, int cnt, float thr) {
   int w = 0;
-  for (int e = 0; e < cnt; e++) {
-    const uint2 x = lg[e];
-    if (__uint_as_float(x.x) <= thr) lg[w++] = x;
+  for (int e = 0; e < cnt; e += 16) {
+    uint2 buf[16];
+#pragma unroll
+    for (int j = 0; j < 16; j++) buf[j] = e + j < cnt ? lg[e + j] : make_uint2(0x7f800000u, 0u);
+#pragma unroll
+    for (int j = 0; j < 16; j++)
+      if (__uint_as_float(buf[j].x) <= thr) lg[w++] = buf[j];
   }
   return w;
 }
@@ -243,11 +265,8 @@ __device__ __forceinline__ void epi_candidate(EpiState &s, float v, uint32_t id,
   const float dp = v + s.qn;
   if (!(dp <= s.thr)) return;
   if (!s.ovf) {
-    if (s.cnt >= logcap) {
-      s.cnt = log_compact(lg, s.cnt, s.thr);
-      if (s.cnt >= logcap) s.ovf = 1;
-    }
-    if (!s.ovf) lg[s.cnt++] = make_uint2(__float_as_uint(dp), id);
+    if (s.cnt < logcap) lg[s.cnt++] = make_uint2(__float_as_uint(dp), id);
+    else s.ovf = 1;
   }
   if (dp < s.root) {
     s.root = heap_replace_root(heap, row, k, dp);
@@ -273,6 +292,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   uint64_t *tfull = bars + 2 * p.NST;
   uint64_t *tempty = bars + 2 * p.NST + 2;
   uint64_t *afull = bars + 2 * p.NST + 4;
+  uint64_t *cnfull = bars + 2 * p.NST + 5;
+  float *cn_s = reinterpret_cast<float *>(smem + L.cn_off);
   uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(smem + L.tmem_off);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -294,6 +315,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       mbar_init(&tempty[b], 4);
     }
     mbar_init(afull, 1);
+    mbar_init(&cnfull[0], 1);
+    mbar_init(&cnfull[1], 1);
     mbar_fence_init();
   }
   if (warp == 1) {
@@ -344,6 +367,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         const int b = lt & 1;
         const uint32_t use = (uint32_t)(lt >> 1);
         if (!mbar_wait(&tempty[b], (use & 1u) ^ 1u)) { failed = true; break; }
+        // buffer b is free, so is its norm slot: fetch this tile's candidate norms
+        mbar_expect_tx(&cnfull[b], (uint32_t)(N * 4));
+        bulk_g2s(cn_s + b * N, p.cn + (size_t)(t_begin + lt) * N, (uint32_t)(N * 4), &cnfull[b]);
         tc_fence_after();
         const uint32_t tmem_d = tmem_base + (uint32_t)(b * N);
         for (int kc = 0; kc < p.nkc; kc++, it++) {
@@ -410,45 +436,71 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       s.Tv = -Num<float>::inf();
     }
     uint2 *lg = p.log + ((size_t)split * p.Q + (valid ? gq : 0)) * p.logcap;
+    // One 32-column chunk: approximate distances, a cheap min-filter, and for the rare chunks
+    // with survivors a warp-convergent pass in which every lane with pending candidates handles
+    // one of them per iteration (selected from its registers by index).
+    auto chunk = [&](const uint32_t (&r)[32], const float *cnt, size_t cbase, int c0) {
+      float v[32];
+      float mn = Num<float>::inf();
+      const float4 *cn4 = reinterpret_cast<const float4 *>(cnt + c0);
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const float4 c4 = cn4[j];
+        v[4 * j + 0] = fmaf(__uint_as_float(r[4 * j + 0]), -2.0f, c4.x);
+        v[4 * j + 1] = fmaf(__uint_as_float(r[4 * j + 1]), -2.0f, c4.y);
+        v[4 * j + 2] = fmaf(__uint_as_float(r[4 * j + 2]), -2.0f, c4.z);
+        v[4 * j + 3] = fmaf(__uint_as_float(r[4 * j + 3]), -2.0f, c4.w);
+      }
+#pragma unroll
+      for (int i = 0; i < 32; i++) mn = fminf(mn, v[i]);
+      if (p.dbg && valid) {
+        for (int i = 0; i < 32; i++) {
+          const long long col = (long long)cbase + c0 + i;
+          if (col < p.dbg_ncols) p.dbg[(size_t)gq * p.dbg_ld + col] = v[i] + s.qn;
+        }
+      }
+      if (!__any_sync(FULL_MASK, mn <= s.Tv)) return;
+      // a chunk appends at most 32 entries per lane: make room first, all lanes together
+      if (__any_sync(FULL_MASK, s.cnt > p.logcap - 32)) {
+        if (s.cnt > p.logcap - 32 && !s.ovf) {
+          s.cnt = log_compact(lg, s.cnt, s.thr);
+          if (s.cnt > p.logcap - 32) s.ovf = 1;
+        }
+      }
+      uint32_t mask = 0;
+      if (mn <= s.Tv) {
+#pragma unroll
+        for (int i = 0; i < 32; i++) mask |= (v[i] <= s.Tv ? 1u : 0u) << i;
+      }
+      while (__any_sync(FULL_MASK, mask != 0)) {
+        if (mask) {
+          const int i = __ffs(mask) - 1;
+          mask &= mask - 1;
+          float x = v[0];
+#pragma unroll
+          for (int j = 1; j < 32; j++) x = (i == j) ? v[j] : x;
+          // the log keeps the packed candidate position; the re-rank maps it to the id
+          epi_candidate(s, x, (uint32_t)(cbase + c0 + i), lg, p.logcap, heap, row, p.k);
+        }
+      }
+    };
     for (int lt = 0; lt < ntile && !failed; lt++) {
       const int b = lt & 1;
       const uint32_t use = (uint32_t)(lt >> 1);
       if (!mbar_wait(&tfull[b], use & 1u)) { failed = true; break; }
+      if (!mbar_wait(&cnfull[b], use & 1u)) { failed = true; break; }
       tc_fence_after();
       const uint32_t taddr = tmem_base + ((uint32_t)(lq * 32) << 16) + (uint32_t)(b * N);
       const int tile = t_begin + lt;
       const size_t cbase = (size_t)tile * N;
-      for (int c0 = 0; c0 < N; c0 += 32) {
-        uint32_t r[32];
+      for (int c0 = 0; c0 < N; c0 += 64) {
+        uint32_t ra[32], rb[32];
         __syncwarp();
-        tmem_ld32(taddr + (uint32_t)c0, r);
+        tmem_ld32(taddr + (uint32_t)c0, ra);
+        tmem_ld32(taddr + (uint32_t)c0 + 32u, rb);
         tmem_wait_ld();
-        float v[32];
-        float mn = Num<float>::inf();
-        const float4 *cn4 = reinterpret_cast<const float4 *>(p.cn + cbase + c0);
-#pragma unroll
-        for (int j = 0; j < 8; j++) {
-          const float4 c4 = __ldg(cn4 + j);
-          v[4 * j + 0] = fmaf(__uint_as_float(r[4 * j + 0]), -2.0f, c4.x);
-          v[4 * j + 1] = fmaf(__uint_as_float(r[4 * j + 1]), -2.0f, c4.y);
-          v[4 * j + 2] = fmaf(__uint_as_float(r[4 * j + 2]), -2.0f, c4.z);
-          v[4 * j + 3] = fmaf(__uint_as_float(r[4 * j + 3]), -2.0f, c4.w);
-        }
-#pragma unroll
-        for (int i = 0; i < 32; i++) mn = fminf(mn, v[i]);
-        if (p.dbg && valid) {
-          for (int i = 0; i < 32; i++) {
-            const long long col = (long long)cbase + c0 + i;
-            if (col < p.dbg_ncols) p.dbg[(size_t)gq * p.dbg_ld + col] = v[i] + s.qn;
-          }
-        }
-        if (mn <= s.Tv) {
-#pragma unroll
-          for (int i = 0; i < 32; i++) {
-            if (v[i] <= s.Tv)
-              epi_candidate(s, v[i], p.cid[cbase + c0 + i], lg, p.logcap, heap, row, p.k);
-          }
-        }
+        chunk(ra, cn_s + b * N, cbase, c0);
+        chunk(rb, cn_s + b * N, cbase, c0 + 32);
       }
       tc_fence_before();
       __syncwarp();
@@ -477,6 +529,7 @@ struct RerankParams {
   const float *margin;
   const float *Xq, *Xq2, *Xc, *Xc2;
   const int *qidx;
+  const uint32_t *cid;  // packed candidate position -> point id
   float *D;
   int *I;
   int ldD;
@@ -575,7 +628,8 @@ __global__ void __launch_bounds__(256) tc_rerank(RerankParams p) {
       while (m) {
         const int j = __ffs(m) - 1;
         m &= m - 1;
-        const uint32_t cid = __shfl_sync(FULL_MASK, ent.y, j);
+        const uint32_t pos = __shfl_sync(FULL_MASK, ent.y, j);
+        const uint32_t cid = p.cid[pos];
         const float *cv = p.Xc + (long long)cid * p.d;
         const double dist = exact_dist_warp(qv, cv, p.d, (double)p.Xc2[cid], qq, lane);
         if (lane == nb) { bd = dist; bi = cid; }
@@ -775,7 +829,7 @@ TcPlan tc_plan(int nq, int nc, int d, int k, int mode, int sms) {
   }
   P.S = best_s;
   P.tiles_per_split = (P.rtiles + P.S - 1) / P.S;
-  P.logcap = std::max(4 * P.kp, 512);
+  P.logcap = std::max(8 * P.kp, 1024);
   // workspace
   size_t off = 0;
   auto take = [&](size_t b) { size_t o = off; off = al256(off + b); return o; };
@@ -846,7 +900,7 @@ cudaError_t tc_run(const TcPlan &P, int nq, int nc, int d, int k, const float *X
   };
   mark("tc_pack", true);
   const int nsample = std::min(nc, 4096);
-  tc_center<<<(d + 127) / 128, 128, 0, st>>>(Xc, d, nrows_c, cidx, nc, nsample, mu, mu2);
+  tc_center<<<(d + 31) / 32, 1024, 0, st>>>(Xc, d, nrows_c, cidx, nc, nsample, mu);
   tc_mu2<<<1, 32, 0, st>>>(mu, d, mu2);
   tc_pack<<<(P.r_pad + 7) / 8, 256, 0, st>>>(P.fmt, Xc, Xc2, d, P.d_pad, nrows_c, cidx, nc,
                                             P.r_pad, mu, mu2, 1, pb, pb_lo, cn, cnrm, cid,
@@ -903,7 +957,7 @@ cudaError_t tc_run(const TcPlan &P, int nq, int nc, int d, int k, const float *X
   RerankParams rp{};
   rp.Q = nq; rp.k = k; rp.S = P.S; rp.logcap = P.logcap; rp.d = d;
   rp.log = tp.log; rp.logcnt = tp.logcnt; rp.kth = tp.kth; rp.margin = tp.margin;
-  rp.Xq = Xq; rp.Xq2 = Xq2; rp.Xc = Xc; rp.Xc2 = Xc2; rp.qidx = qidx;
+  rp.Xq = Xq; rp.Xq2 = Xq2; rp.Xc = Xc; rp.Xc2 = Xc2; rp.qidx = qidx; rp.cid = cid;
   rp.D = D; rp.I = I; rp.ldD = ldD;
   rp.fallback_list = reinterpret_cast<int *>(base + P.o_fbl);
   rp.fallback_count = fbc;
