@@ -67,6 +67,10 @@ def parse():
                     help="headline device run only: no e2e, modes, precision form, CPU baseline")
     ap.add_argument("--precision-only", action="store_true",
                     help="only the precision-form workload (d=256), for profiling")
+    ap.add_argument("--pf-modes", default="fp32,tf32,bf16,bf16x3",
+                    help="modes of the precision-form workload")
+    ap.add_argument("--pf-queries", type=int, default=32768,
+                    help="query count of the precision-form workload (smaller for profiling)")
     ap.add_argument("--cpu-worker", default=None, help=argparse.SUPPRESS)
     return ap.parse_args()
 
@@ -394,17 +398,24 @@ def precision_form(L, G, W, dev, peaks, args):
     """32,768 queries x 262,144 references, d = 256, k = 64, latent-manifold points."""
     import torch
     p = W.config3(seed=3)
-    prob = DeviceProblem(p, p.beta, dev)
-    res = {"workload": "precision form: queries=32768 references=262144 d=256 k=64, "
+    prob = DeviceProblem(p, np.ascontiguousarray(p.beta[:args.pf_queries]), dev)
+    res = {"workload": f"precision form: queries={prob.nq} references=262144 d=256 k=64, "
                        "U[0,1)^8 latent through a seeded orthonormal basis + N(0,1e-3^2)"}
     name2mode = {v: k for k, v in MODE_NAMES.items()}
+    wanted = args.pf_modes.split(",")
     for nm, steps in (("fp32", 2), ("tf32", 5), ("bf16", 5), ("bf16x3", 5)):
-        ms, tr = timed(L, G, prob, name2mode[nm], steps, 1)
+        if nm not in wanted:
+            continue
+        if args.precision_only and args.profile_only:
+            steps = 1
+        ms, tr = timed(L, G, prob, name2mode[nm], steps, 0 if args.profile_only else 1)
         res[nm] = {"ms_per_step": ms, "value": prob.evals / (ms * 1e-3),
                    "roofline": roofline(nm, prob, tr, peaks, None), "kernels": tr}
-    base = res["fp32"]["value"]
-    for nm in ("tf32", "bf16", "bf16x3"):
-        res[nm]["speedup_vs_plain_fp32"] = res[nm]["value"] / base
+    if "fp32" in res:
+        base = res["fp32"]["value"]
+        for nm in ("tf32", "bf16", "bf16x3"):
+            if nm in res:
+                res[nm]["speedup_vs_plain_fp32"] = res[nm]["value"] / base
     del prob
     torch.cuda.empty_cache()
     return res

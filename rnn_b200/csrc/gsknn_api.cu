@@ -307,8 +307,33 @@ static int knn_device_tc(int mode, int nq, int nc, int d, int k, const float *Xq
   CU(scratch(SLOT_STATUS, 256, st, &stv));
   int *status = static_cast<int *>(stv);
   CU(cudaMemsetAsync(status, 0, sizeof(int), st));
+  // GSKNN_TC_COUNTERS=1: per-call diagnostics of the tensor-core epilogue on stderr
+  static const bool want_counters = std::getenv("GSKNN_TC_COUNTERS") != nullptr;
+  unsigned long long *counters = nullptr;
+  if (want_counters) {
+    void *cv = nullptr;
+    CU(scratch(SLOT_AUX, 64, st, &cv));
+    counters = static_cast<unsigned long long *>(cv);
+    CU(cudaMemsetAsync(counters, 0, 64, st));
+  }
   CU(tc_run(P, nq, nc, d, k, Xq, Xq2, nrows_q, qidx, Xc, Xc2, nrows_c, cidx, D, I, ldD, ws,
-            status, dbg, dbg_ld, st, trace_hook, nullptr));
+            status, dbg, dbg_ld, counters, st, trace_hook, nullptr));
+  if (counters) {
+    unsigned long long h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int nfb = 0;
+    CU(cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(&nfb, static_cast<char *>(ws) + P.o_fbc, sizeof(int),
+                       cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    std::fprintf(stderr,
+                 "gsknn tc: mode=%d n=%d m=%d d=%d k=%d S=%d N=%d: logged/query=%.1f "
+                 "inserts/query=%.1f loop-iters/warp=%.1f slow-chunks/warp=%.1f "
+                 "chunks/warp=%.1f rerank-scanned/query=%.1f exact/query=%.1f fallback=%d\n",
+                 mode, nq, nc, d, k, P.S, P.N, (double)h[0] / nq, (double)h[1] / nq,
+                 (double)h[2] / (P.qtiles * P.S * 8.0), (double)h[3] / (P.qtiles * P.S * 8.0),
+                 (double)h[4] / (P.qtiles * P.S * 8.0), (double)h[5] / nq, (double)h[6] / nq,
+                 nfb);
+  }
   if (margin)
     CU(cudaMemcpyAsync(margin, static_cast<char *>(ws) + P.o_margin, (size_t)nq * 4,
                        cudaMemcpyDeviceToDevice, st));

@@ -79,7 +79,7 @@ struct TcPlan {
   unsigned smem;
   float coefA, coefB;
   size_t o_mu, o_mu2, o_stats, o_pa, o_pa_lo, o_pb, o_pb_lo, o_qn, o_qnrm, o_cn, o_cnrm,
-      o_cid, o_log, o_logcnt, o_kth, o_margin, o_fbl, o_fbc;
+      o_cid, o_log, o_logcnt, o_kth, o_kth_shared, o_margin, o_fbl, o_fbc;
   size_t bytes;
 };
 
@@ -88,6 +88,7 @@ cudaError_t tc_run(const TcPlan &P, int nq, int nc, int d, int k, const float *X
                    const float *Xq2, long long nrows_q, const int *qidx, const float *Xc,
                    const float *Xc2, long long nrows_c, const int *cidx, float *D, int *I,
                    int ldD, void *ws, int *status, float *dbg, long long dbg_ld,
-                   cudaStream_t st, TraceHook hook, void *hook_ctx);
+                   unsigned long long *counters, cudaStream_t st, TraceHook hook,
+                   void *hook_ctx);
 
 }  // namespace gsknn

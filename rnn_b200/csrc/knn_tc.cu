@@ -39,7 +39,11 @@ namespace tc {
 constexpr int TC_M = 128;            // queries per CTA (TMEM lanes)
 constexpr int CHUNK_BYTES = 128;     // K bytes per TMA box / swizzle atom row
 constexpr int A_CHUNK = TC_M * CHUNK_BYTES;  // 16 KB
-constexpr int NTHREADS = 192;        // producer, MMA, 4 epilogue warps
+// Warp 0 TMA producer, warp 1 MMA issuer, warps 2-9 epilogue: two warps per TMEM lane quarter,
+// the first of each pair (the heap owner) taking the low half of every tile's columns and the
+// second (log only) the high half.
+constexpr int NEPI = 8;
+constexpr int NTHREADS = 32 * (2 + NEPI);
 constexpr uint32_t LOG_OVF = 1u << 30;
 
 // ------------------------------------------------------------------------------------------
@@ -179,11 +183,13 @@ struct TcParams {
   uint2 *log;
   int *logcnt;
   float *kth;
+  unsigned *kth_shared;  // per query: best k-th approximate distance over splits (float bits)
   float *margin;
   int *status;
   float *dbg;
   long long dbg_ld;
   long long dbg_ncols;
+  unsigned long long *counters;  // optional diagnostics (5 counters), may be null
 };
 
 struct SmemLayout {
@@ -213,13 +219,19 @@ __host__ __device__ inline SmemLayout tc_smem_layout(int nkc, int a_terms, int b
 }
 
 struct EpiState {
-  float qn, E2, thr0, root, thr, Tv;
+  float qn, E2, thr0, root, shared, thr, Tv;
   int cnt;
   int ovf;
+  // optional diagnostics: logged candidates, heap inserts, convergent-loop iterations, chunks
+  // that took the slow path
+  unsigned n_ev, n_ins, n_it, n_sc;
 };
 
+// The k-th smallest approximate distance of any subset of the candidates bounds the global one
+// from above, so the threshold uses the smaller of this split's own k-th and the best one any
+// split of the query has published.
 __device__ __forceinline__ void refresh_threshold(EpiState &s) {
-  float t = s.root + s.E2;
+  float t = fminf(s.root, s.shared) + s.E2;
   s.thr = t < s.thr0 ? t : s.thr0;
   // filter in the v = d' - qn' space with slack for the rounding of the subtraction
   s.Tv = (s.thr - s.qn) + (fabsf(s.thr) + fabsf(s.qn)) * 2.4e-7f + 1e-30f;
@@ -261,15 +273,23 @@ __device__ __noinline__ int log_compact(uint2 *lg, int cnt, float thr) {
 }
 
 __device__ __forceinline__ void epi_candidate(EpiState &s, float v, uint32_t id, uint2 *lg,
-                                              int logcap, float *heap, int row, int k) {
+                                              int logcap, float *heap, int row, int k,
+                                              unsigned *ksh) {
   const float dp = v + s.qn;
   if (!(dp <= s.thr)) return;
+  s.n_ev++;
   if (!s.ovf) {
     if (s.cnt < logcap) lg[s.cnt++] = make_uint2(__float_as_uint(dp), id);
     else s.ovf = 1;
   }
-  if (dp < s.root) {
+  if (ksh && dp < s.root) {  // heap owners only (ksh == nullptr: log-only warp)
+    s.n_ins++;
     s.root = heap_replace_root(heap, row, k, dp);
+    // publish to the other splits (non-negative floats order like their bit patterns)
+    if (s.root >= 0.0f && s.root < s.shared) {
+      atomicMin(ksh, __float_as_uint(s.root));
+      s.shared = s.root;
+    }
     refresh_threshold(s);
   }
 }
@@ -312,7 +332,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     }
     for (int b = 0; b < 2; b++) {
       mbar_init(&tfull[b], 1);
-      mbar_init(&tempty[b], 4);
+      mbar_init(&tempty[b], NEPI);
     }
     mbar_init(afull, 1);
     mbar_init(&cnfull[0], 1);
@@ -404,14 +424,20 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     }
   } else {
     // ---------------- epilogue: one query row per thread ----------------
-    const int lq = warp & 3;  // TMEM lane quarter this warp may access
+    const int lq = warp & 3;            // TMEM lane quarter this warp may access
+    const int half = (warp - 2) >> 2;   // 0: heap owner, low columns; 1: log only, high columns
+    const bool owner = half == 0;
     const int row = lq * 32 + lane;
     const int gq = qt * TC_M + row;
     const bool valid = gq < p.Q;
-    for (int i = 0; i < p.k; i++) heap[i * TC_M + row] = Num<float>::inf();
+    if (owner)
+      for (int i = 0; i < p.k; i++) heap[i * TC_M + row] = Num<float>::inf();
     EpiState s;
     s.cnt = 0;
     s.ovf = 0;
+    s.shared = Num<float>::inf();
+    s.n_ev = s.n_ins = s.n_it = s.n_sc = 0;
+    unsigned *ksh = p.kth_shared + (valid ? gq : 0);
     s.root = Num<float>::inf();
     s.qn = 0.0f;
     s.E2 = 0.0f;
@@ -430,12 +456,13 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         if (mx > -Num<float>::inf()) s.thr0 = mx + s.E2;
       }
       refresh_threshold(s);
-      if (split == 0) p.margin[gq] = s.E2;
+      if (split == 0 && owner) p.margin[gq] = s.E2;
     } else {
       s.thr = -Num<float>::inf();
       s.Tv = -Num<float>::inf();
     }
-    uint2 *lg = p.log + ((size_t)split * p.Q + (valid ? gq : 0)) * p.logcap;
+    const int lslot = 2 * split + half;  // this warp's log among the 2S logs of the query
+    uint2 *lg = p.log + ((size_t)lslot * p.Q + (valid ? gq : 0)) * p.logcap;
     // One 32-column chunk: approximate distances, a cheap min-filter, and for the rare chunks
     // with survivors a warp-convergent pass in which every lane with pending candidates handles
     // one of them per iteration (selected from its registers by index).
@@ -451,8 +478,17 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         v[4 * j + 2] = fmaf(__uint_as_float(r[4 * j + 2]), -2.0f, c4.z);
         v[4 * j + 3] = fmaf(__uint_as_float(r[4 * j + 3]), -2.0f, c4.w);
       }
+      {
+        // tree minimum: depth 5 instead of a 32-long dependency chain
+        float m16[16];
 #pragma unroll
-      for (int i = 0; i < 32; i++) mn = fminf(mn, v[i]);
+        for (int j = 0; j < 16; j++) m16[j] = fminf(v[2 * j], v[2 * j + 1]);
+#pragma unroll
+        for (int w = 8; w >= 1; w >>= 1)
+#pragma unroll
+          for (int j = 0; j < w; j++) m16[j] = fminf(m16[2 * j], m16[2 * j + 1]);
+        mn = m16[0];
+      }
       if (p.dbg && valid) {
         for (int i = 0; i < 32; i++) {
           const long long col = (long long)cbase + c0 + i;
@@ -472,28 +508,45 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 #pragma unroll
         for (int i = 0; i < 32; i++) mask |= (v[i] <= s.Tv ? 1u : 0u) << i;
       }
+      s.n_sc++;
       while (__any_sync(FULL_MASK, mask != 0)) {
+        s.n_it++;
         if (mask) {
           const int i = __ffs(mask) - 1;
           mask &= mask - 1;
-          float x = v[0];
+          // v[i] for a runtime i: a 5-level select tree on the bits of i
+          float t16[16];
 #pragma unroll
-          for (int j = 1; j < 32; j++) x = (i == j) ? v[j] : x;
+          for (int j = 0; j < 16; j++) t16[j] = (i & 16) ? v[j + 16] : v[j];
+#pragma unroll
+          for (int w = 8, bit = 8; w >= 1; w >>= 1, bit >>= 1)
+#pragma unroll
+            for (int j = 0; j < w; j++) t16[j] = (i & bit) ? t16[j + w] : t16[j];
           // the log keeps the packed candidate position; the re-rank maps it to the id
-          epi_candidate(s, x, (uint32_t)(cbase + c0 + i), lg, p.logcap, heap, row, p.k);
+          epi_candidate(s, t16[0], (uint32_t)(cbase + c0 + i), lg, p.logcap, heap, row, p.k,
+                        owner ? ksh : nullptr);
         }
       }
     };
     for (int lt = 0; lt < ntile && !failed; lt++) {
       const int b = lt & 1;
       const uint32_t use = (uint32_t)(lt >> 1);
+      if (valid) {
+        // pick up what the query's other splits have found (all bits set = nothing yet)
+        const float sh = __uint_as_float(__ldcg(ksh));
+        if (sh < s.shared) {
+          s.shared = sh;
+          refresh_threshold(s);
+        }
+      }
       if (!mbar_wait(&tfull[b], use & 1u)) { failed = true; break; }
       if (!mbar_wait(&cnfull[b], use & 1u)) { failed = true; break; }
       tc_fence_after();
       const uint32_t taddr = tmem_base + ((uint32_t)(lq * 32) << 16) + (uint32_t)(b * N);
       const int tile = t_begin + lt;
       const size_t cbase = (size_t)tile * N;
-      for (int c0 = 0; c0 < N; c0 += 64) {
+      const int cb = half * (N / 2), ce = cb + N / 2;
+      for (int c0 = cb; c0 < ce; c0 += 64) {
         uint32_t ra[32], rb[32];
         __syncwarp();
         tmem_ld32(taddr + (uint32_t)c0, ra);
@@ -507,8 +560,17 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       if (lane == 0) mbar_arrive(&tempty[b]);
     }
     if (valid) {
-      p.kth[(size_t)split * p.Q + gq] = s.root;
-      p.logcnt[(size_t)split * p.Q + gq] = s.cnt | (s.ovf ? (int)LOG_OVF : 0);
+      p.kth[(size_t)lslot * p.Q + gq] = s.root;  // +inf for log-only warps
+      p.logcnt[(size_t)lslot * p.Q + gq] = s.cnt | (s.ovf ? (int)LOG_OVF : 0);
+    }
+    if (p.counters) {
+      atomicAdd(&p.counters[0], (unsigned long long)s.n_ev);
+      atomicAdd(&p.counters[1], (unsigned long long)s.n_ins);
+      if (lane == 0) {
+        atomicAdd(&p.counters[2], (unsigned long long)s.n_it);
+        atomicAdd(&p.counters[3], (unsigned long long)s.n_sc);
+        atomicAdd(&p.counters[4], (unsigned long long)ntile * (N / 64));
+      }
     }
   }
   if (failed) atomicExch(p.status, GSKNN_ERR_TIMEOUT);
@@ -526,6 +588,7 @@ struct RerankParams {
   const uint2 *log;
   const int *logcnt;
   const float *kth;
+  const unsigned *kth_shared;
   const float *margin;
   const float *Xq, *Xq2, *Xc, *Xc2;
   const int *qidx;
@@ -535,10 +598,33 @@ struct RerankParams {
   int ldD;
   int *fallback_list;
   int *fallback_count;
+  unsigned long long *counters;  // optional: [5] entries scanned, [6] exact distances
 };
 
 // Exact squared distance of the oracle: (-2 <q,c> + |c|^2) + |q|^2 in FP64 from float inputs,
 // clamped at zero; the dot product is split across the warp.
+// The same distance computed by one thread: the FP64 dot product accumulates the (exact)
+// float x float products in dimension order, as the oracle does (frame/dgsknn_ref_impl.h).
+__device__ __forceinline__ double exact_dist_lane(const float *q, const float *c, int d,
+                                                  double cc, double qq) {
+  double acc = 0.0;
+  if ((d & 3) == 0 && ((reinterpret_cast<uintptr_t>(q) | reinterpret_cast<uintptr_t>(c)) & 15) == 0) {
+    const float4 *q4 = reinterpret_cast<const float4 *>(q);
+    const float4 *c4 = reinterpret_cast<const float4 *>(c);
+    for (int i = 0; i < (d >> 2); i++) {
+      const float4 a = __ldg(q4 + i), b = __ldg(c4 + i);
+      acc = fma((double)a.x, (double)b.x, acc);
+      acc = fma((double)a.y, (double)b.y, acc);
+      acc = fma((double)a.z, (double)b.z, acc);
+      acc = fma((double)a.w, (double)b.w, acc);
+    }
+  } else {
+    for (int pp = 0; pp < d; pp++) acc = fma((double)q[pp], (double)c[pp], acc);
+  }
+  const double v = fma(-2.0, acc, cc) + qq;
+  return v < 0.0 ? 0.0 : v;
+}
+
 __device__ __forceinline__ double exact_dist_warp(const float *q, const float *c, int d,
                                                   double cc, double qq, int lane) {
   double acc = 0.0;
@@ -582,12 +668,13 @@ __device__ __forceinline__ void load_heap_row(const float *D, const int *I, int 
 
 template <int E>
 __global__ void __launch_bounds__(256) tc_rerank(RerankParams p) {
+  __shared__ uint32_t rr_stage[8][64];
   const int lane = threadIdx.x & 31;
   const int q = blockIdx.x * 8 + (threadIdx.x >> 5);
   if (q >= p.Q) return;
   // overflowed logs: the whole query goes to the brute-force pass
   bool ovf = false;
-  float T = Num<float>::inf();
+  float T = __uint_as_float(p.kth_shared[q]);  // NaN (all bits set) when nothing was published
   for (int s = 0; s < p.S; s++) {
     ovf |= (p.logcnt[(size_t)s * p.Q + q] & (int)LOG_OVF) != 0;
     T = fminf(T, p.kth[(size_t)s * p.Q + q]);
@@ -597,6 +684,37 @@ __global__ void __launch_bounds__(256) tc_rerank(RerankParams p) {
     return;
   }
   const float E2 = p.margin[q];
+  // Pass 1: the exact k-th smallest approximate distance over all of the query's logs. Every
+  // candidate among the k smallest approximate distances was logged (its d' was below every
+  // threshold in force), so this is the global approximate k-th, usually far below the bound T
+  // the splits ended with.
+  {
+    float kd[E];
+    uint32_t ki[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) { kd[e] = Num<float>::inf(); ki[e] = NO_ID; }
+    float kth = T;
+    for (int s = 0; s < p.S; s++) {
+      const int cnt = p.logcnt[(size_t)s * p.Q + q];
+      const uint2 *lg = p.log + ((size_t)s * p.Q + q) * p.logcap;
+      for (int base = 0; base < cnt; base += 32) {
+        const int e = base + lane;
+        float dv = Num<float>::inf();
+        if (e < cnt) dv = __uint_as_float(lg[e].x);
+        if (!__any_sync(FULL_MASK, dv <= kth)) continue;
+        float b1[1] = {dv};
+        uint32_t i1[1] = {(uint32_t)e};
+        warp_sort<float, 1>(b1, i1, lane);
+        warp_merge_32<float, E>(kd, ki, b1[0], i1[0], lane);
+        float t = kd[0];
+#pragma unroll
+        for (int e2 = 0; e2 < E; e2++)
+          if (e2 == (p.k - 1) / 32) t = kd[e2];
+        kth = fminf(kth, __shfl_sync(FULL_MASK, t, (p.k - 1) & 31));
+      }
+    }
+    T = kth;
+  }
   float thr = T + E2;
   {
     float mx = -Num<float>::inf();
@@ -610,12 +728,28 @@ __global__ void __launch_bounds__(256) tc_rerank(RerankParams p) {
   const long long qrow = p.qidx[q];
   const float *qv = p.Xq + qrow * p.d;
   const double qq = (double)p.Xq2[qrow];
-  double bd = Num<double>::inf();
-  uint32_t bi = NO_ID;
+  // Pass 2: band entries are compacted into a per-warp staging list; every 32 of them each lane
+  // computes one exact distance (independent row gathers across the lanes), then the batch is
+  // sorted and merged into the exact list.
+  uint32_t *stg = rr_stage[threadIdx.x >> 5];
   int nb = 0;
+  auto flush = [&](int count) {
+    double dist = Num<double>::inf();
+    uint32_t id = NO_ID;
+    if (lane < count) {
+      id = p.cid[stg[lane]];
+      dist = exact_dist_lane(qv, p.Xc + (long long)id * p.d, p.d, (double)p.Xc2[id], qq);
+    }
+    if (p.counters && lane == 0) atomicAdd(&p.counters[6], (unsigned long long)count);
+    double b1[1] = {dist};
+    uint32_t i1[1] = {id};
+    warp_sort<double, 1>(b1, i1, lane);
+    warp_merge_32<double, E>(ld, li, b1[0], i1[0], lane);
+  };
   for (int s = 0; s < p.S; s++) {
     const int cnt = p.logcnt[(size_t)s * p.Q + q];
     const uint2 *lg = p.log + ((size_t)s * p.Q + q) * p.logcap;
+    if (p.counters && lane == 0) atomicAdd(&p.counters[5], (unsigned long long)cnt);
     for (int base = 0; base < cnt; base += 32) {
       const int e = base + lane;
       uint2 ent = make_uint2(0u, NO_ID);
@@ -624,33 +758,22 @@ __global__ void __launch_bounds__(256) tc_rerank(RerankParams p) {
         ent = lg[e];
         take = __uint_as_float(ent.x) <= thr;
       }
-      unsigned m = __ballot_sync(FULL_MASK, take);
-      while (m) {
-        const int j = __ffs(m) - 1;
-        m &= m - 1;
-        const uint32_t pos = __shfl_sync(FULL_MASK, ent.y, j);
-        const uint32_t cid = p.cid[pos];
-        const float *cv = p.Xc + (long long)cid * p.d;
-        const double dist = exact_dist_warp(qv, cv, p.d, (double)p.Xc2[cid], qq, lane);
-        if (lane == nb) { bd = dist; bi = cid; }
-        if (++nb == 32) {
-          double b1[1] = {bd};
-          uint32_t i1[1] = {bi};
-          warp_sort<double, 1>(b1, i1, lane);
-          warp_merge_32<double, E>(ld, li, b1[0], i1[0], lane);
-          bd = Num<double>::inf();
-          bi = NO_ID;
-          nb = 0;
-        }
+      const unsigned m = __ballot_sync(FULL_MASK, take);
+      if (take) stg[nb + __popc(m & ((1u << lane) - 1u))] = ent.y;
+      nb += __popc(m);
+      __syncwarp();
+      if (nb >= 32) {
+        flush(32);
+        __syncwarp();
+        const uint32_t rest = lane < nb - 32 ? stg[32 + lane] : 0u;
+        __syncwarp();
+        if (lane < nb - 32) stg[lane] = rest;
+        nb -= 32;
+        __syncwarp();
       }
     }
   }
-  if (nb > 0) {
-    double b1[1] = {bd};
-    uint32_t i1[1] = {bi};
-    warp_sort<double, 1>(b1, i1, lane);
-    warp_merge_32<double, E>(ld, li, b1[0], i1[0], lane);
-  }
+  if (nb > 0) flush(nb);
   write_heap_row<E>(p.D, p.I, p.ldD, q, p.k, ld, li, lane);
 }
 
@@ -824,7 +947,8 @@ TcPlan tc_plan(int nq, int nc, int d, int k, int mode, int sms) {
   double best = 1e300;
   for (int s = 1; s <= std::min(P.rtiles, 16); s++) {
     const long long items = (long long)P.qtiles * s;
-    const double cost = (double)((items + sms - 1) / sms) / s * (1.0 + 0.01 * s);
+    // each split pays a start-up burst before the shared threshold tightens
+    const double cost = (double)((items + sms - 1) / sms) / s * (1.0 + 0.03 * s);
     if (cost < best - 1e-12) { best = cost; best_s = s; }
   }
   P.S = best_s;
@@ -845,9 +969,11 @@ TcPlan tc_plan(int nq, int nc, int d, int k, int mode, int sms) {
   P.o_cn = take((size_t)P.r_pad * 4);
   P.o_cnrm = take((size_t)P.r_pad * 4);
   P.o_cid = take((size_t)P.r_pad * 4);
-  P.o_log = take((size_t)P.S * nq * P.logcap * 8);
-  P.o_logcnt = take((size_t)P.S * nq * 4);
-  P.o_kth = take((size_t)P.S * nq * 4);
+  // two logs per (query, split): one per epilogue warp of a lane quarter
+  P.o_log = take((size_t)2 * P.S * nq * P.logcap * 8);
+  P.o_logcnt = take((size_t)2 * P.S * nq * 4);
+  P.o_kth = take((size_t)2 * P.S * nq * 4);
+  P.o_kth_shared = take((size_t)nq * 4);
   P.o_margin = take((size_t)nq * 4);
   P.o_fbl = take((size_t)nq * 4);
   P.o_fbc = take(16);
@@ -874,7 +1000,8 @@ cudaError_t tc_run(const TcPlan &P, int nq, int nc, int d, int k, const float *X
                    const float *Xq2, long long nrows_q, const int *qidx, const float *Xc,
                    const float *Xc2, long long nrows_c, const int *cidx, float *D, int *I,
                    int ldD, void *ws, int *status, float *dbg, long long dbg_ld,
-                   cudaStream_t st, TraceHook hook, void *hook_ctx) {
+                   unsigned long long *counters, cudaStream_t st, TraceHook hook,
+                   void *hook_ctx) {
   using namespace tc;
   char *base = static_cast<char *>(ws);
   float *mu = reinterpret_cast<float *>(base + P.o_mu);
@@ -893,6 +1020,7 @@ cudaError_t tc_run(const TcPlan &P, int nq, int nc, int d, int k, const float *X
   cudaError_t e;
   e = cudaMemsetAsync(stats, 0, 16, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(fbc, 0, 16, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(base + P.o_kth_shared, 0xFF, (size_t)nq * 4, st);
   if (e != cudaSuccess) return e;
 
   auto mark = [&](const char *name, bool begin) {
@@ -933,11 +1061,13 @@ cudaError_t tc_run(const TcPlan &P, int nq, int nc, int d, int k, const float *X
   tp.log = reinterpret_cast<uint2 *>(base + P.o_log);
   tp.logcnt = reinterpret_cast<int *>(base + P.o_logcnt);
   tp.kth = reinterpret_cast<float *>(base + P.o_kth);
+  tp.kth_shared = reinterpret_cast<unsigned *>(base + P.o_kth_shared);
   tp.margin = reinterpret_cast<float *>(base + P.o_margin);
   tp.status = status;
   tp.dbg = dbg;
   tp.dbg_ld = dbg_ld;
   tp.dbg_ncols = nc;
+  tp.counters = counters;
   dim3 grid(P.qtiles, P.S);
   mark("tc_knn", true);
   if (P.fmt == 0) {
@@ -955,12 +1085,14 @@ cudaError_t tc_run(const TcPlan &P, int nq, int nc, int d, int k, const float *X
   if (e != cudaSuccess) return e;
 
   RerankParams rp{};
-  rp.Q = nq; rp.k = k; rp.S = P.S; rp.logcap = P.logcap; rp.d = d;
+  rp.Q = nq; rp.k = k; rp.S = 2 * P.S; rp.logcap = P.logcap; rp.d = d;
   rp.log = tp.log; rp.logcnt = tp.logcnt; rp.kth = tp.kth; rp.margin = tp.margin;
+  rp.kth_shared = tp.kth_shared;
   rp.Xq = Xq; rp.Xq2 = Xq2; rp.Xc = Xc; rp.Xc2 = Xc2; rp.qidx = qidx; rp.cid = cid;
   rp.D = D; rp.I = I; rp.ldD = ldD;
   rp.fallback_list = reinterpret_cast<int *>(base + P.o_fbl);
   rp.fallback_count = fbc;
+  rp.counters = counters;
   FallbackParams fp{};
   fp.k = k; fp.d = d; fp.nc = nc; fp.Xq = Xq; fp.Xq2 = Xq2; fp.Xc = Xc; fp.Xc2 = Xc2;
   fp.qidx = qidx; fp.cidx = cidx; fp.nrows_c = nrows_c; fp.D = D; fp.I = I; fp.ldD = ldD;
