@@ -233,6 +233,10 @@ struct EpiState {
 __device__ __forceinline__ void refresh_threshold(EpiState &s) {
   float t = fminf(s.root, s.shared) + s.E2;
   s.thr = t < s.thr0 ? t : s.thr0;
+  if (s.thr == -Num<float>::inf()) {  // padding rows past the last query: never admit
+    s.Tv = -Num<float>::inf();
+    return;
+  }
   // filter in the v = d' - qn' space with slack for the rounding of the subtraction
   s.Tv = (s.thr - s.qn) + (fabsf(s.thr) + fabsf(s.qn)) * 2.4e-7f + 1e-30f;
 }
@@ -272,9 +276,13 @@ __device__ __noinline__ int log_compact(uint2 *lg, int cnt, float thr) {
   return w;
 }
 
+constexpr int PEND = 8;  // heap inserts a lane may defer before the warp flushes them
+
+// Log the candidate and, for heap owners, defer its heap insert into a small register ring
+// (filled through compile-time indices so it stays in registers).
 __device__ __forceinline__ void epi_candidate(EpiState &s, float v, uint32_t id, uint2 *lg,
-                                              int logcap, float *heap, int row, int k,
-                                              unsigned *ksh) {
+                                              int logcap, bool owner, float (&pend)[PEND],
+                                              int &np) {
   const float dp = v + s.qn;
   if (!(dp <= s.thr)) return;
   s.n_ev++;
@@ -282,16 +290,32 @@ __device__ __forceinline__ void epi_candidate(EpiState &s, float v, uint32_t id,
     if (s.cnt < logcap) lg[s.cnt++] = make_uint2(__float_as_uint(dp), id);
     else s.ovf = 1;
   }
-  if (ksh && dp < s.root) {  // heap owners only (ksh == nullptr: log-only warp)
-    s.n_ins++;
-    s.root = heap_replace_root(heap, row, k, dp);
-    // publish to the other splits (non-negative floats order like their bit patterns)
-    if (s.root >= 0.0f && s.root < s.shared) {
-      atomicMin(ksh, __float_as_uint(s.root));
-      s.shared = s.root;
-    }
-    refresh_threshold(s);
+  if (owner && dp < s.root) {
+#pragma unroll
+    for (int j = 0; j < PEND; j++)
+      if (j == np) pend[j] = dp;
+    np++;
   }
+}
+
+// Apply the deferred inserts (all lanes of the warp together, so their sift-downs overlap),
+// publish the new k-th to the other splits and tighten the threshold.
+__device__ __forceinline__ void epi_flush(EpiState &s, float *heap, int row, int k,
+                                          float (&pend)[PEND], int &np, unsigned *ksh) {
+#pragma unroll
+  for (int j = 0; j < PEND; j++) {
+    if (j < np && pend[j] < s.root) {
+      s.n_ins++;
+      s.root = heap_replace_root(heap, row, k, pend[j]);
+    }
+  }
+  np = 0;
+  // non-negative floats order like their bit patterns
+  if (s.root >= 0.0f && s.root < s.shared) {
+    atomicMin(ksh, __float_as_uint(s.root));
+    s.shared = s.root;
+  }
+  refresh_threshold(s);
 }
 
 template <int FMT>
@@ -438,6 +462,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     s.shared = Num<float>::inf();
     s.n_ev = s.n_ins = s.n_it = s.n_sc = 0;
     unsigned *ksh = p.kth_shared + (valid ? gq : 0);
+    float pend[PEND];
+    int np = 0;
+#pragma unroll
+    for (int j = 0; j < PEND; j++) pend[j] = Num<float>::inf();
     s.root = Num<float>::inf();
     s.qn = 0.0f;
     s.E2 = 0.0f;
@@ -458,6 +486,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       refresh_threshold(s);
       if (split == 0 && owner) p.margin[gq] = s.E2;
     } else {
+      // padding row: its log and shared-bound pointers alias query 0, so it must never admit a
+      // candidate; the -inf ceiling survives every threshold refresh
+      s.thr0 = -Num<float>::inf();
       s.thr = -Num<float>::inf();
       s.Tv = -Num<float>::inf();
     }
@@ -505,8 +536,17 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       }
       uint32_t mask = 0;
       if (mn <= s.Tv) {
+        // pass mask as an OR tree (depth 5)
+        uint32_t m16[16];
 #pragma unroll
-        for (int i = 0; i < 32; i++) mask |= (v[i] <= s.Tv ? 1u : 0u) << i;
+        for (int j = 0; j < 16; j++)
+          m16[j] = (v[2 * j] <= s.Tv ? 1u << (2 * j) : 0u) |
+                   (v[2 * j + 1] <= s.Tv ? 1u << (2 * j + 1) : 0u);
+#pragma unroll
+        for (int w = 8; w >= 1; w >>= 1)
+#pragma unroll
+          for (int j = 0; j < w; j++) m16[j] = m16[2 * j] | m16[2 * j + 1];
+        mask = m16[0];
       }
       s.n_sc++;
       while (__any_sync(FULL_MASK, mask != 0)) {
@@ -523,21 +563,26 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 #pragma unroll
             for (int j = 0; j < w; j++) t16[j] = (i & bit) ? t16[j + w] : t16[j];
           // the log keeps the packed candidate position; the re-rank maps it to the id
-          epi_candidate(s, t16[0], (uint32_t)(cbase + c0 + i), lg, p.logcap, heap, row, p.k,
-                        owner ? ksh : nullptr);
+          epi_candidate(s, t16[0], (uint32_t)(cbase + c0 + i), lg, p.logcap, owner, pend, np);
+        }
+        if (__any_sync(FULL_MASK, np == PEND)) {
+          if (owner) epi_flush(s, heap, row, p.k, pend, np, ksh);
         }
       }
     };
+    // what the query's other splits have found (all bits set = nothing yet); the load for the
+    // next tile is issued a tile ahead so its latency hides behind the tile's work
+    unsigned sh_next = valid ? __ldcg(ksh) : 0xFFFFFFFFu;
     for (int lt = 0; lt < ntile && !failed; lt++) {
       const int b = lt & 1;
       const uint32_t use = (uint32_t)(lt >> 1);
       if (valid) {
-        // pick up what the query's other splits have found (all bits set = nothing yet)
-        const float sh = __uint_as_float(__ldcg(ksh));
+        const float sh = __uint_as_float(sh_next);
         if (sh < s.shared) {
           s.shared = sh;
           refresh_threshold(s);
         }
+        sh_next = __ldcg(ksh);
       }
       if (!mbar_wait(&tfull[b], use & 1u)) { failed = true; break; }
       if (!mbar_wait(&cnfull[b], use & 1u)) { failed = true; break; }
@@ -559,6 +604,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       __syncwarp();
       if (lane == 0) mbar_arrive(&tempty[b]);
     }
+    if (owner) epi_flush(s, heap, row, p.k, pend, np, ksh);
     if (valid) {
       p.kth[(size_t)lslot * p.Q + gq] = s.root;  // +inf for log-only warps
       p.logcnt[(size_t)lslot * p.Q + gq] = s.cnt | (s.ovf ? (int)LOG_OVF : 0);
