@@ -351,6 +351,35 @@ static int pick_mode(int nq, int nc, int d, int k) {
 }
 
 template <typename T>
+int knn_device_large(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, long long nrows_q,
+                     const int *qidx, const T *Xc, const T *Xc2, long long nrows_c,
+                     const int *cidx, T *D, int *I, int ldD, int four_ary, cudaStream_t st) {
+  if (nq == 0 || nc == 0 || d == 0 || k == 0)
+    return set_status(GSKNN_EARLY_RETURN, "early return: m, n, d or k is 0");
+  const int need = four_ary ? k + KNN_HEAP_OFFSET : k;
+  if (nq < 0 || nc < 0 || d < 0 || k < 0 || ldD < need)
+    return set_status(GSKNN_ERR_ARG, "invalid sizes (n=%d m=%d d=%d k=%d ldD=%d)", nq, nc, d,
+                      k, ldD);
+  if (!Xq || !Xq2 || !qidx || !Xc || !Xc2 || !cidx || !D || !I)
+    return set_status(GSKNN_ERR_ARG, "null pointer argument");
+  if (large_select_smem(k, sizeof(T)) > 227 * 1024)
+    return set_status(GSKNN_ERR_UNSUPPORTED, "k=%d exceeds the selection kernel (k <= %d)", k,
+                      sizeof(T) == 8 ? 16384 : 16384);
+  const LargePlan P = large_plan<T>(nq, nc, d, k, (size_t)1 << 30);
+  void *ws = nullptr, *stv = nullptr;
+  CU(scratch(SLOT_KERNEL, P.bytes, st, &ws));
+  CU(scratch(SLOT_STATUS, 256, st, &stv));
+  int *status = static_cast<int *>(stv);
+  CU(cudaMemsetAsync(status, 0, sizeof(int), st));
+  {
+    TraceScope ts("select_rows", st);
+    CU(large_run<T>(P, nq, nc, d, k, Xq, Xq2, nrows_q, qidx, Xc, Xc2, nrows_c, cidx, D, I, ldD,
+                    four_ary, ws, status, st));
+  }
+  return set_status(GSKNN_OK, nullptr);
+}
+
+template <typename T>
 int knn_device(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, long long nrows_q,
                const int *qidx, const T *Xc, const T *Xc2, long long nrows_c, const int *cidx,
                T *D, int *I, int ldD, cudaStream_t st) {
@@ -360,6 +389,10 @@ int knn_device(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, long lon
       return knn_device_tc(mode, nq, nc, d, k, Xq, Xq2, nrows_q, qidx, Xc, Xc2, nrows_c, cidx,
                            D, I, ldD, st);
   }
+  // lists beyond the fused kernels' capacity: explicit distance block + row selection
+  if (simt_geometry<T>(k).kp == 0)
+    return knn_device_large<T>(nq, nc, d, k, Xq, Xq2, nrows_q, qidx, Xc, Xc2, nrows_c, cidx, D,
+                               I, ldD, 0, st);
   return knn_device_simt<T>(nq, nc, d, k, Xq, Xq2, nrows_q, qidx, Xc, Xc2, nrows_c, cidx, D, I,
                             ldD, st);
 }
@@ -395,11 +428,13 @@ static bool index_range(const int *idx, int n, int *lo, int *hi) {
 }
 
 template <typename T>
+// path: 0 = the default dispatch, 1 = explicit distance block + selection into binary heaps,
+// 2 = the same into 4-ary heaps with the 3-slot header (rows of ldD >= k + 3).
 int knn_host(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, const int *qidx,
-             const T *Xc, const T *Xc2, const int *cidx, T *D, int *I, int ldD) {
+             const T *Xc, const T *Xc2, const int *cidx, T *D, int *I, int ldD, int path = 0) {
   if (nq == 0 || nc == 0 || d == 0 || k == 0)
     return set_status(GSKNN_EARLY_RETURN, "early return: m, n, d or k is 0");
-  if (nq < 0 || nc < 0 || d < 0 || k < 0 || ldD < k)
+  if (nq < 0 || nc < 0 || d < 0 || k < 0 || ldD < (path == 2 ? k + KNN_HEAP_OFFSET : k))
     return set_status(GSKNN_ERR_ARG, "invalid sizes");
   if (!Xq || !Xq2 || !qidx || !Xc || !Xc2 || !cidx || !D || !I)
     return set_status(GSKNN_ERR_ARG, "null pointer argument");
@@ -444,9 +479,15 @@ int knn_host(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, const int 
   CU(cudaMemcpyAsync(pci, cidx, (size_t)nc * 4, cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync(pD, D, (size_t)nq * ldD * sizeof(T), cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync(pI, I, (size_t)nq * ldD * 4, cudaMemcpyHostToDevice, st));
-  rc = knn_device<T>(nq, nc, d, k, dXq, dXq2, (long long)qhi + 1, static_cast<int *>(pqi),
-                     dXc, dXc2, (long long)chi + 1, static_cast<int *>(pci),
-                     static_cast<T *>(pD), static_cast<int *>(pI), ldD, st);
+  if (path == 0)
+    rc = knn_device<T>(nq, nc, d, k, dXq, dXq2, (long long)qhi + 1, static_cast<int *>(pqi),
+                       dXc, dXc2, (long long)chi + 1, static_cast<int *>(pci),
+                       static_cast<T *>(pD), static_cast<int *>(pI), ldD, st);
+  else
+    rc = knn_device_large<T>(nq, nc, d, k, dXq, dXq2, (long long)qhi + 1,
+                             static_cast<int *>(pqi), dXc, dXc2, (long long)chi + 1,
+                             static_cast<int *>(pci), static_cast<T *>(pD),
+                             static_cast<int *>(pI), ldD, path == 2 ? 1 : 0, st);
   if (rc != GSKNN_OK) {
     cudaStreamSynchronize(st);
     return rc;
@@ -455,6 +496,56 @@ int knn_host(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, const int 
   if (rc != GSKNN_OK) return rc;
   CU(cudaMemcpyAsync(D, pD, (size_t)nq * ldD * sizeof(T), cudaMemcpyDeviceToHost, st));
   CU(cudaMemcpyAsync(I, pI, (size_t)nq * ldD * 4, cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  return set_status(GSKNN_OK, nullptr);
+}
+
+// Distance block of host tables: C[j*ldc + i] for rows j < nq (qidx) and columns i < nc (cidx).
+template <typename T>
+int sq2nrm_host(int nq, int nc, int d, const T *Xq, const T *Xq2, const int *qidx, const T *Xc,
+                const T *Xc2, const int *cidx, T *C, int ldc) {
+  if (nq == 0 || nc == 0 || d == 0)
+    return set_status(GSKNN_EARLY_RETURN, "early return: m, n or k is 0");
+  if (nq < 0 || nc < 0 || d < 0 || ldc < nc)
+    return set_status(GSKNN_ERR_ARG, "invalid sizes (ldc must be >= m)");
+  if (!Xq || !Xq2 || !qidx || !Xc || !Xc2 || !cidx || !C)
+    return set_status(GSKNN_ERR_ARG, "null pointer argument");
+  int qlo, qhi, clo, chi;
+  if (!index_range(qidx, nq, &qlo, &qhi) || !index_range(cidx, nc, &clo, &chi))
+    return set_status(GSKNN_ERR_INDEX, "negative point index");
+  cudaStream_t st = host_stream();
+  const size_t qrows = (size_t)(qhi - qlo + 1), crows = (size_t)(chi - clo + 1);
+  void *pq, *pq2, *pc, *pc2, *pqi, *pci, *pC, *stv, *ws;
+  CU(scratch(SLOT_HQTAB, qrows * d * sizeof(T), st, &pq));
+  CU(scratch(SLOT_HQNRM, qrows * sizeof(T), st, &pq2));
+  CU(scratch(SLOT_HCTAB, crows * d * sizeof(T), st, &pc));
+  CU(scratch(SLOT_HCNRM, crows * sizeof(T), st, &pc2));
+  CU(scratch(SLOT_HQIDX, (size_t)nq * 4, st, &pqi));
+  CU(scratch(SLOT_HCIDX, (size_t)nc * 4, st, &pci));
+  CU(scratch(SLOT_HD, (size_t)nq * nc * sizeof(T), st, &pC));
+  CU(scratch(SLOT_STATUS, 256, st, &stv));
+  CU(cudaMemcpyAsync(pq, Xq + (size_t)qlo * d, qrows * d * sizeof(T), cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(pq2, Xq2 + qlo, qrows * sizeof(T), cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(pc, Xc + (size_t)clo * d, crows * d * sizeof(T), cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(pc2, Xc2 + clo, crows * sizeof(T), cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(pqi, qidx, (size_t)nq * 4, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(pci, cidx, (size_t)nc * 4, cudaMemcpyHostToDevice, st));
+  int *status = static_cast<int *>(stv);
+  CU(cudaMemsetAsync(status, 0, sizeof(int), st));
+  const LargePlan P = large_plan<T>(nq, nc, d, 1, 0);
+  CU(scratch(SLOT_KERNEL, P.bytes, st, &ws));
+  {
+    TraceScope ts("dist_block", st);
+    CU(block_run<T>(P, nq, nc, d, static_cast<const T *>(pq) - (size_t)qlo * d,
+                    static_cast<const T *>(pq2) - qlo, (long long)qhi + 1,
+                    static_cast<const int *>(pqi), static_cast<const T *>(pc) - (size_t)clo * d,
+                    static_cast<const T *>(pc2) - clo, (long long)chi + 1,
+                    static_cast<const int *>(pci), static_cast<T *>(pC), nc, ws, status, st));
+  }
+  int rc = device_status(st);
+  if (rc != GSKNN_OK) return rc;
+  CU(cudaMemcpy2DAsync(C, (size_t)ldc * sizeof(T), pC, (size_t)nc * sizeof(T),
+                       (size_t)nc * sizeof(T), (size_t)nq, cudaMemcpyDeviceToHost, st));
   CU(cudaStreamSynchronize(st));
   return set_status(GSKNN_OK, nullptr);
 }
@@ -582,32 +673,40 @@ void dgsknn(int m, int n, int k, int r, double *XA, double *XA2, int *alpha, dou
   knn_host<double>(n, m, k, r, XB, XB2, beta, XA, XA2, alpha, heap->D, heap->I, heap->ldk);
 }
 
+// frame/gsknn.c:597-659. The heap's own layout decides the selection: 4-ary with the header
+// when heapCreate_d built it that way (heap->d == 4), binary otherwise (attached heaps).
 void dgsknn_var3(int m, int n, int k, int r, double *XA, double *XA2, int *amap, double *XB,
                  double *XB2, int *bmap, heap_t *heap) {
-  (void)m; (void)n; (void)k; (void)r; (void)XA; (void)XA2; (void)amap; (void)XB; (void)XB2;
-  (void)bmap; (void)heap;
-  set_status(GSKNN_ERR_UNSUPPORTED, "dgsknn_var3: large-k path not built yet");
+  if (!heap) {
+    set_status(GSKNN_ERR_ARG, "null heap");
+    return;
+  }
+  knn_host<double>(n, m, k, r, XB, XB2, bmap, XA, XA2, amap, heap->D, heap->I, heap->ldk,
+                   heap->d == 4 ? 2 : 1);
 }
 
 void dgssq2nrm(int m, int n, int k, double *XA, double *XA2, int *amap, double *XB,
                double *XB2, int *bmap, double *C, int ldc) {
-  (void)m; (void)n; (void)k; (void)XA; (void)XA2; (void)amap; (void)XB; (void)XB2; (void)bmap;
-  (void)C; (void)ldc;
-  set_status(GSKNN_ERR_UNSUPPORTED, "dgssq2nrm: not built yet");
+  sq2nrm_host<double>(n, m, k, XB, XB2, bmap, XA, XA2, amap, C, ldc);
 }
 
+// frame/gsknn_ref.c:63-162: D/I are n rows of r (binary heaps), candidates on the alpha side.
 void sgsknn_ref(int m, int n, int k, int r, float *XA, float *XA2, int *alpha, float *XB,
                 float *XB2, int *beta, float *D, int *I) {
-  (void)m; (void)n; (void)k; (void)r; (void)XA; (void)XA2; (void)alpha; (void)XB; (void)XB2;
-  (void)beta; (void)D; (void)I;
-  set_status(GSKNN_ERR_UNSUPPORTED, "sgsknn_ref: not built yet");
+  if (r == 0) {
+    set_status(GSKNN_EARLY_RETURN, "early return: r is 0");
+    return;
+  }
+  knn_host<float>(n, m, k, r, XB, XB2, beta, XA, XA2, alpha, D, I, r, 1);
 }
 
 void dgsknn_ref(int m, int n, int k, int r, double *XA, double *XA2, int *alpha, double *XB,
                 double *XB2, int *beta, double *D, int *I) {
-  (void)m; (void)n; (void)k; (void)r; (void)XA; (void)XA2; (void)alpha; (void)XB; (void)XB2;
-  (void)beta; (void)D; (void)I;
-  set_status(GSKNN_ERR_UNSUPPORTED, "dgsknn_ref: not built yet");
+  if (r == 0) {
+    set_status(GSKNN_EARLY_RETURN, "early return: r is 0");
+    return;
+  }
+  knn_host<double>(n, m, k, r, XB, XB2, beta, XA, XA2, alpha, D, I, r, 1);
 }
 
 }  // extern "C"

@@ -63,6 +63,25 @@ cudaError_t launch_simt(const SimtArgs<T> &a, int kp, int qtiles, int S, cudaStr
 template <typename T>
 cudaError_t launch_finalize(const FinalizeArgs<T> &a, int kp, cudaStream_t st);
 
+// ---- explicit distance block + per-row selection (large k, var3, dgssq2nrm, *_ref) ----------
+struct LargePlan {
+  int nkc, qtiles, rtiles, chunk_rows;
+  size_t o_ap, o_bp, o_qn, o_cn, o_cid, o_c, bytes, sel_smem;
+};
+template <typename T>
+LargePlan large_plan(int nq, int nc, int d, int k, size_t max_block_bytes);
+size_t large_select_smem(int k, size_t elem);
+template <typename T>
+cudaError_t large_run(const LargePlan &P, int nq, int nc, int d, int k, const T *Xq,
+                      const T *Xq2, long long nrows_q, const int *qidx, const T *Xc,
+                      const T *Xc2, long long nrows_c, const int *cidx, T *D, int *I, int ldD,
+                      int four_ary, void *ws, int *status, cudaStream_t st);
+template <typename T>
+cudaError_t block_run(const LargePlan &P, int nq, int nc, int d, const T *Xq, const T *Xq2,
+                      long long nrows_q, const int *qidx, const T *Xc, const T *Xc2,
+                      long long nrows_c, const int *cidx, T *Cout, long long ldc, void *ws,
+                      int *status, cudaStream_t st);
+
 // ---- tensor-core (tcgen05) precision form, float inputs ------------------------------------
 // Arithmetic formats of the approximate pass (the public GSKNN_MODE_* values map onto them).
 #define GSKNN_TC_TF32 2
