@@ -108,6 +108,7 @@ static void release_all_for_device(int dev) {
 struct TraceRec {
   const char *name;
   cudaEvent_t a, b;
+  int nk;  // kernels of the library launched between a and b
 };
 static std::mutex g_tmu;
 static bool g_trace = false;
@@ -128,8 +129,9 @@ static cudaEvent_t ev_get() {
 struct TraceScope {
   const char *name;
   cudaStream_t st;
+  int nk;
   cudaEvent_t a = nullptr;
-  TraceScope(const char *n, cudaStream_t s) : name(n), st(s) {
+  TraceScope(const char *n, cudaStream_t s, int kernels = 1) : name(n), st(s), nk(kernels) {
     if (!g_trace) return;
     std::lock_guard<std::mutex> lk(g_tmu);
     a = ev_get();
@@ -140,7 +142,7 @@ struct TraceScope {
     std::lock_guard<std::mutex> lk(g_tmu);
     cudaEvent_t b = ev_get();
     cudaEventRecord(b, st);
-    g_recs.push_back({name, a, b});
+    g_recs.push_back({name, a, b, nk});
   }
 };
 
@@ -183,7 +185,7 @@ static int choose_splits(int qtiles, int rtiles, int slots) {
 }
 
 // Tracer hook for pipelines that bracket groups of launches themselves (the tensor-core path).
-static void trace_hook(void *, const char *name, bool begin, cudaStream_t st) {
+static void trace_hook(void *, const char *name, bool begin, cudaStream_t st, int nkernels) {
   if (!g_trace) return;
   std::lock_guard<std::mutex> lk(g_tmu);
   static thread_local std::vector<std::pair<const char *, cudaEvent_t>> pending;
@@ -197,7 +199,7 @@ static void trace_hook(void *, const char *name, bool begin, cudaStream_t st) {
     if (std::strcmp(pending[i].first, name) == 0) {
       cudaEvent_t b = ev_get();
       cudaEventRecord(b, st);
-      g_recs.push_back({name, pending[i].second, b});
+      g_recs.push_back({name, pending[i].second, b, nkernels});
       pending.erase(pending.begin() + (long)i);
       return;
     }
@@ -372,7 +374,8 @@ int knn_device_large(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, lo
   int *status = static_cast<int *>(stv);
   CU(cudaMemsetAsync(status, 0, sizeof(int), st));
   {
-    TraceScope ts("select_rows", st);
+    // two packing launches, then a distance block and a selection per chunk of query rows
+    TraceScope ts("select_rows", st, 2 + 2 * ((nq + P.chunk_rows - 1) / P.chunk_rows));
     CU(large_run<T>(P, nq, nc, d, k, Xq, Xq2, nrows_q, qidx, Xc, Xc2, nrows_c, cidx, D, I, ldD,
                     four_ary, ws, status, st));
   }
@@ -535,7 +538,7 @@ int sq2nrm_host(int nq, int nc, int d, const T *Xq, const T *Xq2, const int *qid
   const LargePlan P = large_plan<T>(nq, nc, d, 1, 0);
   CU(scratch(SLOT_KERNEL, P.bytes, st, &ws));
   {
-    TraceScope ts("dist_block", st);
+    TraceScope ts("dist_block", st, 3);  // two packing launches and the distance block
     CU(block_run<T>(P, nq, nc, d, static_cast<const T *>(pq) - (size_t)qlo * d,
                     static_cast<const T *>(pq2) - qlo, (long long)qhi + 1,
                     static_cast<const int *>(pqi), static_cast<const T *>(pc) - (size_t)clo * d,
@@ -612,7 +615,7 @@ int gsknn_trace_read(char *buf, int len) {
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
       Acc &x = acc[r.name];
-      x.n++;
+      x.n += r.nk;
       x.ms += ms;
     }
     g_evpool.push_back(r.a);

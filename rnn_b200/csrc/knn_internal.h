@@ -88,8 +88,10 @@ cudaError_t block_run(const LargePlan &P, int nq, int nc, int d, const T *Xq, co
 #define GSKNN_TC_BF16 3
 #define GSKNN_TC_BF16X3 4
 
-// Kernel-launch bracket used by the library's tracer (begin/end around a group of launches).
-typedef void (*TraceHook)(void *ctx, const char *name, bool begin, cudaStream_t st);
+// Kernel-launch bracket used by the library's tracer (begin/end around a group of launches);
+// `nkernels` (read at the end) counts the library's own kernels launched inside the bracket.
+typedef void (*TraceHook)(void *ctx, const char *name, bool begin, cudaStream_t st,
+                          int nkernels);
 
 struct TcPlan {
   bool ok;

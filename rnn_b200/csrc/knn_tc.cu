@@ -1069,8 +1069,9 @@ cudaError_t tc_run(const TcPlan &P, int nq, int nc, int d, int k, const float *X
   if (e == cudaSuccess) e = cudaMemsetAsync(base + P.o_kth_shared, 0xFF, (size_t)nq * 4, st);
   if (e != cudaSuccess) return e;
 
-  auto mark = [&](const char *name, bool begin) {
-    if (hook) hook(hook_ctx, name, begin, st);
+  // tracer brackets; `nk` = kernels of this file launched inside the bracket
+  auto mark = [&](const char *name, bool begin, int nk = 0) {
+    if (hook) hook(hook_ctx, name, begin, st, nk);
   };
   mark("tc_pack", true);
   const int nsample = std::min(nc, 4096);
@@ -1083,7 +1084,7 @@ cudaError_t tc_run(const TcPlan &P, int nq, int nc, int d, int k, const float *X
                                             P.q_pad, mu, mu2, 0, pa, pa_lo, qn, qnrm, nullptr,
                                             stats, status);
   e = cudaGetLastError();
-  mark("tc_pack", false);
+  mark("tc_pack", false, 4);  // centre, mu.mu, two packs
   if (e != cudaSuccess) return e;
 
   CUtensorMap mA, mAlo, mB, mBlo;
@@ -1127,7 +1128,7 @@ cudaError_t tc_run(const TcPlan &P, int nq, int nc, int d, int k, const float *X
     if (e == cudaSuccess) tc_knn<2><<<grid, NTHREADS, P.smem, st>>>(mA, mAlo, mB, mBlo, tp);
   }
   if (e == cudaSuccess) e = cudaGetLastError();
-  mark("tc_knn", false);
+  mark("tc_knn", false, 1);
   if (e != cudaSuccess) return e;
 
   RerankParams rp{};
@@ -1153,7 +1154,7 @@ cudaError_t tc_run(const TcPlan &P, int nq, int nc, int d, int k, const float *X
     default: return cudaErrorInvalidValue;
   }
   e = cudaGetLastError();
-  mark("tc_rerank", false);
+  mark("tc_rerank", false, 2);  // re-rank and fallback
   return e;
 }
 
