@@ -19,6 +19,11 @@ seeded; the reference publishes no dataset for this path.
 `precision_form`: the precision workload (32,768 queries x 262,144 references, d = 256, k = 64,
            points on an 8-dim latent manifold + noise): TF32 / BF16 tensor-core + FP64 re-rank
            against the plain FP32 kernel, with the tensor pipe's roofline.
+`batching_form`: all-nearest-neighbour search over randomized-tree leaves (N = 2,097,152 points
+           of the same kind of mixture, d = 64, k = 32, 8 trees per pass, leaves of 256..2048
+           points, alpha = beta = leaf, 4 passes merged into one heap): every leaf of a pass in
+           one persistent launch replayed from a CUDA graph, tile shape by the autotuner;
+           distance evaluations (sum of leaf sizes squared) per second over the 4 passes.
 `roofline`: the dominant kernel of the headline run; contraction counted as 2d flops per
            evaluation, against the measured bf16 dense peak (MEASURED_PEAKS.json; half of it
            for TF32, the TF32 tensor rate) or, for the CUDA-core kernel, the FP32 issue rate at
@@ -71,6 +76,12 @@ def parse():
                     help="modes of the precision-form workload")
     ap.add_argument("--pf-queries", type=int, default=32768,
                     help="query count of the precision-form workload (smaller for profiling)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batching-form workload")
+    ap.add_argument("--batch-only", action="store_true",
+                    help="only the batching-form workload (all-NN over tree leaves)")
+    ap.add_argument("--batch-points", type=int, default=1 << 21,
+                    help="points of the batching-form workload (smaller for profiling)")
+    ap.add_argument("--batch-passes", type=int, default=4)
     ap.add_argument("--cpu-worker", default=None, help=argparse.SUPPRESS)
     return ap.parse_args()
 
@@ -96,6 +107,9 @@ def cpu_worker(spec: str) -> None:
     os.environ["OMP_NUM_THREADS"] = str(nthreads)
     os.environ["GSKNN_IC_NT"] = str(nthreads)
     from rnn_b200 import workloads as W
+    if cfg.get("kind") == "batch":
+        batch_cpu_worker(cfg, nthreads)
+        return
     p = W.config2(seed=cfg["seed"])
     ref_so = os.path.join(ROOT, "oracle", "_ref", "libgsknn_ref.so")
     kind = "reference" if os.path.exists(ref_so) else "port"
@@ -127,6 +141,50 @@ def cpu_worker(spec: str) -> None:
         t = run(q)
     out = {"value": q * p.m / t, "seconds": t, "queries": q, "kind": kind, "threads": nthreads}
     print("CPUJSON " + json.dumps(out), flush=True)
+
+
+def batch_cpu_worker(cfg, nthreads) -> None:
+    """The reference's sgsknn once per leaf (alpha = beta = leaf), as its tree drivers run it,
+    over the leaves of one tree of the batching workload until the time target is reached."""
+    from rnn_b200 import batch as B
+    from rnn_b200 import workloads as W
+    from oracle.oracle import ReferenceLib
+    ref_so = os.path.join(ROOT, "oracle", "_ref", "libgsknn_ref.so")
+    p = W.config4(seed=cfg["seed"], n_points=cfg["points"])
+    lv = B.rkdt_leaves(p.X, 1, p.leaf_min, p.leaf_max, seed=p.tree_seed)
+    R = ReferenceLib(ref_so)
+    evals, t, n = 0.0, 0.0, 0
+    for l in range(lv.nleaves):
+        leaf = np.ascontiguousarray(lv.pts[lv.ptr[l]:lv.ptr[l + 1]])
+        D = np.full((leaf.size, p.k), 1.79e30, dtype=np.float32)
+        I = np.full((leaf.size, p.k), -1, dtype=np.int32)
+        t0 = time.perf_counter()
+        R.var1(p.k, p.X, p.X2, leaf, p.X, p.X2, leaf, D, I)
+        t += time.perf_counter() - t0
+        evals += float(leaf.size) ** 2
+        n += 1
+        if t >= cfg["seconds"]:
+            break
+    print("CPUJSON " + json.dumps({"value": evals / t, "seconds": t, "leaves": n,
+                                   "kind": "reference", "threads": nthreads}), flush=True)
+
+
+def batch_cpu_baseline(seconds: float, threads: int, points: int) -> dict:
+    spec = json.dumps({"kind": "batch", "threads": threads, "seconds": seconds, "seed": 4,
+                       "points": points})
+    env = dict(os.environ)
+    env["CUDA_VISIBLE_DEVICES"] = ""
+    r = subprocess.run([sys.executable, os.path.abspath(__file__), "--cpu-worker", spec],
+                       capture_output=True, text=True, env=env, timeout=900)
+    for line in r.stdout.splitlines():
+        if line.startswith("CPUJSON "):
+            o = json.loads(line[8:])
+            return {"value": o["value"], "unit": "distance-evals/s", "cores": o["threads"],
+                    "kind": o["kind"],
+                    "sample": (f"reference sgsknn_var1 per leaf (alpha = beta = leaf), "
+                               f"{o['leaves']} leaves of one tree, {o['seconds']:.1f} s, "
+                               f"GSKNN_IC_NT=OMP_NUM_THREADS={o['threads']}")}
+    raise RuntimeError("batch cpu baseline failed:\n" + r.stdout[-2000:] + r.stderr[-2000:])
 
 
 def cpu_baseline(seconds: float, threads: int) -> dict:
@@ -324,6 +382,8 @@ def run_ours(args, rank, world, local_rank):
             dist.barrier()
 
     out = {}
+    if args.batch_only:
+        return batching_form(L, G, W, dev, peaks, args, args.threads)
     if not args.precision_only:
         p = W.config2(seed=2)
         nq = args.queries
@@ -380,6 +440,8 @@ def run_ours(args, rank, world, local_rank):
         if args.precision_only:
             return pf
         out["precision_form"] = pf
+        if not args.no_batch and not args.profile_only:
+            out["batching_form"] = batching_form(L, G, W, dev, peaks, args, args.threads)
     G.set_mode(0)
     return out
 
@@ -418,6 +480,74 @@ def precision_form(L, G, W, dev, peaks, args):
                 res[nm]["speedup_vs_plain_fp32"] = res[nm]["value"] / base
     del prob
     torch.cuda.empty_cache()
+    return res
+
+
+def batching_form(L, G, W, dev, peaks, args, threads):
+    """All-NN over randomized-tree leaves: 8 trees per pass x 4 passes, one persistent
+    graph-replayed launch per pass."""
+    import torch
+    from rnn_b200 import batch as B
+    p = W.config4(seed=4, n_points=args.batch_points, passes=args.batch_passes)
+    T = p.trees_per_pass
+    t0 = time.perf_counter()
+    lv = B.rkdt_leaves(p.X, T * p.passes, p.leaf_min, p.leaf_max, seed=p.tree_seed)
+    t_build = time.perf_counter() - t0
+    passes = [lv.tree_range(i * T, (i + 1) * T) for i in range(p.passes)]
+    evals = [float((np.diff(q.ptr).astype(np.float64) ** 2).sum()) for q in passes]
+    Xd = torch.from_numpy(p.X).to(dev)
+    X2d = torch.from_numpy(p.X2).to(dev)
+    D = torch.full((p.N, p.k), float("inf"), device=dev)
+    I = torch.full((p.N, p.k), -1, dtype=torch.int32, device=dev)
+    st = torch.cuda.current_stream(dev)
+    B.forget_tuning()
+    job = B.BatchJob(Xd, X2d, D, I, p.k, T, p.leaf_min, shape=-1, stream=st)
+    # warm-up: the first pass tunes the tile shape on its leaves and captures the graph
+    job.run_pass(passes[0])
+    job.sync()
+    tune = job.info()
+    D.fill_(float("inf"))
+    I.fill_(-1)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(st)
+    for q in passes:
+        job.run_pass(q)
+    ev1.record(st)
+    job.sync()
+    ms = ev0.elapsed_time(ev1)
+    info = job.info()
+    job.close()
+    total = sum(evals)
+    sm_mhz = 1965.0
+    peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    achieved = total * (2 * p.d + 3) / (ms * 1e-3) / 1e12
+    res = {
+        "workload": p.name, "points": p.N, "d": p.d, "k": p.k, "trees_per_pass": T,
+        "passes": p.passes, "leaves_per_pass": [int(q.nleaves) for q in passes],
+        "evals_per_pass": evals, "tree_build_s": round(t_build, 2),
+        "ms_total": ms, "ms_per_pass": ms / p.passes,
+        "value": total / (ms * 1e-3), "unit": "distance-evals/s",
+        "dtype": "f32 CUDA-core distances (sgsknn arithmetic)",
+        "launch": {"tile_shape": info["shape_name"], "tile_rows": info["tile_rows"],
+                   "persistent_grid": info["grid"], "work_items_last_pass": info["items"],
+                   "autotune_ms": tune["tune_ms"], "cuda_graph": True,
+                   "kernels_per_pass": 3},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "peak_source": "nominal FP32 CUDA-core issue rate at 1965 MHz",
+                     "note": "whole pass (pack + leaves + merge), 2d+3 flops per evaluation"},
+    }
+    del Xd, X2d, D, I
+    torch.cuda.empty_cache()
+    if not args.no_cpu_baseline:
+        try:
+            res["cpu_baseline"] = batch_cpu_baseline(max(5.0, args.cpu_seconds / 2), threads,
+                                                     args.batch_points)
+            res["speedup_vs_cpu"] = res["value"] / res["cpu_baseline"]["value"]
+        except Exception as e:  # reported, not fatal
+            res["cpu_baseline"] = {"error": str(e)[-400:]}
     return res
 
 
@@ -490,9 +620,10 @@ def main():
         from datetime import timedelta
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    args.threads = threads
     out = run_ours(args, rank, world, local_rank)
     if (rank == 0 and world == 1 and not args.no_cpu_baseline and not args.profile_only
-            and not args.precision_only):
+            and not args.precision_only and not args.batch_only):
         try:
             out["cpu_baseline"] = cpu_baseline(args.cpu_seconds, threads)
         except Exception as e:  # reported, not fatal

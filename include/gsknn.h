@@ -222,6 +222,56 @@ int gsknn_trace_read(char *buf, int len);
 /* Frees the library's cached device scratch memory of the current device. */
 void gsknn_release_workspace(void);
 
+/* ---- Batching form: all-nearest-neighbour search over randomized-tree leaves ---------------
+ * No counterpart in the reference, whose tree drivers (frame/old/dgsrnn_directKQuery.cpp and
+ * the rnn tree code) call dgsknn once per leaf with alpha = beta = the leaf's point list.
+ *
+ * A job owns device buffers for N points (table X, norms X2: device pointers, float) and
+ * updates the caller's device heap D / I (N rows, row stride ldD >= k, initialised by the
+ * caller, e.g. +inf / -1). Each pass takes the leaves of up to `trees_per_pass` trees over the
+ * same points as host CSR arrays: leaf l holds leaf_pts[leaf_ptr[l] .. leaf_ptr[l+1]) and
+ * belongs to tree leaf_tree[l] (a point appears at most once per tree). For every leaf, every
+ * point of the leaf gets the leaf's points as candidates (itself included, at distance 0);
+ * the pass's lists are merged into the heap with duplicates removed, so the heap converges to
+ * the k nearest among every leaf-mate seen in any pass. Arithmetic: FP32 on the CUDA cores as
+ * in sgsknn (ties to the lower id); rows are written in descending order (valid max-heaps).
+ *
+ * One pass is one persistent launch over all leaves (work items dealt by an atomic counter,
+ * longest first), packed and merged by two more kernels, captured once in a CUDA graph and
+ * replayed for every pass on `stream`. `leaf_min` bounds the smallest leaf (it sizes the
+ * buffers); `shape` picks the tile shape (0: 128-row tiles, 1 and 2: 64-row tiles) or, with
+ * -1, lets the autotuner time every shape on the first pass of each (d, k, mean leaf size)
+ * class and remember the fastest for the process. Passes are asynchronous: gsknn_batch_pass
+ * returns once the pass is enqueued (it waits only for the previous pass's plan upload);
+ * gsknn_batch_sync waits and reports index errors. */
+typedef struct gsknn_batch_s gsknn_batch_t;
+gsknn_batch_t *gsknn_batch_create(int N, int d, int k, const float *X, const float *X2,
+                                  float *D, int *I, int ldD, int trees_per_pass, int leaf_min,
+                                  int shape, void *stream);
+int gsknn_batch_pass(gsknn_batch_t *job, const int *leaf_ptr, const int *leaf_pts,
+                     const int *leaf_tree, int nleaves);
+int gsknn_batch_sync(gsknn_batch_t *job);
+/* Shape in use, its tile rows, persistent grid, tiles / work items / distance evaluations of
+ * the last pass, and (when this job ran the autotuner) the trial time of each shape in ms
+ * (-1: not tried). Any pointer may be NULL. */
+int gsknn_batch_info(const gsknn_batch_t *job, int *shape, int *tile_rows, int *grid,
+                     int *tiles, int *items, double *evals, float *tune_ms);
+void gsknn_batch_destroy(gsknn_batch_t *job);
+/* Forgets every tile shape the autotuner has chosen in this process. */
+void gsknn_batch_forget_tuning(void);
+
+/* Randomized projection trees on the host (the caller side of the batching form): `ntrees`
+ * trees over the N x d row-major float points X. Each tree first draws leaf sizes uniformly in
+ * [leaf_min, leaf_max] (leaf_max >= 2 leaf_min) that sum to N, then splits every node along a
+ * random Gaussian direction at the rank that separates its leaves into two halves of nearly
+ * equal size. Output: leaf_ptr (capacity max_leaves + 1), leaf_pts (ntrees * N entries),
+ * leaf_tree (capacity max_leaves), *nleaves. Trees are built in parallel (`threads`, 0 = all
+ * cores); the result depends only on `seed`. Returns 0, or GSKNN_ERR_ARG / GSKNN_ERR_UNSUPPORTED
+ * (capacity too small). */
+int gsknn_rkdt_leaves(const float *X, int N, int d, int ntrees, int leaf_min, int leaf_max,
+                      unsigned long long seed, int threads, int *leaf_ptr, int *leaf_pts,
+                      int *leaf_tree, int max_leaves, int *nleaves);
+
 #ifdef __cplusplus
 }
 #endif

@@ -375,6 +375,69 @@ void oracle_select_rows_d(int m, int n, int k, const double *C, int ldc, const i
 }
 
 /* ------------------------------------------------------------------------------------------
+ * Batching form: union of leaf-mates per point, de-duplicated, exact FP64 selection.
+ * ---------------------------------------------------------------------------------------- */
+void oracle_allnn_leaves_s(int N, int d, int k, const float *X, const float *X2, int nleaves,
+                           const int *ptr, const int *pts, const float *Din, const int *Iin,
+                           int ldin, double *Dout, int *Iout) {
+  if (N <= 0 || k <= 0) return;
+  /* leaves of every point (CSR inversion) */
+  int *cnt = (int *)calloc((size_t)N + 1, sizeof(int));
+  for (int l = 0; l < nleaves; l++)
+    for (int t = ptr[l]; t < ptr[l + 1]; t++) cnt[pts[t] + 1]++;
+  for (int p = 0; p < N; p++) cnt[p + 1] += cnt[p];
+  int *fill = (int *)malloc(sizeof(int) * (size_t)N);
+  memcpy(fill, cnt, sizeof(int) * (size_t)N);
+  int *mine = (int *)malloc(sizeof(int) * (size_t)(cnt[N] > 0 ? cnt[N] : 1));
+  for (int l = 0; l < nleaves; l++)
+    for (int t = ptr[l]; t < ptr[l + 1]; t++) mine[fill[pts[t]]++] = l;
+  int nt = nthreads_for((long)N * 256 * d);
+#pragma omp parallel num_threads(nt)
+  {
+    entry_t *h = (entry_t *)malloc(sizeof(entry_t) * (size_t)k);
+    int *seen = (int *)malloc(sizeof(int) * (size_t)N);
+    for (int i = 0; i < N; i++) seen[i] = -1;
+#pragma omp for schedule(dynamic, 16)
+    for (int p = 0; p < N; p++) {
+      int c = 0;
+      const float *b = X + (size_t)p * d;
+      const double bb = (double)X2[p];
+      for (int u = cnt[p]; u < cnt[p + 1]; u++) {
+        const int l = mine[u];
+        for (int t = ptr[l]; t < ptr[l + 1]; t++) {
+          const int q = pts[t];
+          if (seen[q] == p) continue;
+          seen[q] = p;
+          const float *a = X + (size_t)q * d;
+          double dot = 0.0;
+          for (int j = 0; j < d; j++) dot += (double)a[j] * (double)b[j];
+          double v = -2.0 * dot + (double)X2[q] + bb;
+          if (!(v >= 0.0)) v = v < 0.0 ? 0.0 : v;
+          if (v != v) v = INFINITY;
+          entry_t e = {v, (uint32_t)q};
+          ent_push_bounded(h, &c, k, e);
+        }
+      }
+      if (Din) {
+        for (int t = 0; t < k; t++) {
+          const int q = Iin[(size_t)p * ldin + t];
+          if (q >= 0 && q < N && seen[q] == p) continue; /* already taken from a leaf */
+          if (q >= 0 && q < N) seen[q] = p;
+          entry_t e = {(double)Din[(size_t)p * ldin + t], (uint32_t)q};
+          ent_push_bounded(h, &c, k, e);
+        }
+      }
+      finish_row(h, c, k, Dout + (size_t)p * k, Iout + (size_t)p * k);
+    }
+    free(seen);
+    free(h);
+  }
+  free(mine);
+  free(fill);
+  free(cnt);
+}
+
+/* ------------------------------------------------------------------------------------------
  * Heap validity.
  * ---------------------------------------------------------------------------------------- */
 int oracle_is_maxheap_d(int n, int k, int ld, const double *D) {

@@ -79,6 +79,16 @@ void oracle_select_rows_d(int m, int n, int k, const double *C, int ldc, const i
                           const double *Din, const int *Iin, int ldin,
                           double *Dout, int *Iout);
 
+/* Batching form (no reference function; restates what the reference's tree drivers obtain by
+ * calling sgsknn once per leaf with alpha = beta = the leaf, frame/gsknn.c:1106-1135, plus the
+ * removal of neighbours found twice): for every point p < N, the k nearest (FP64 distances of
+ * the float inputs as in oracle_knn_exact_s, clamped, lower id first on ties) among the union
+ * of p's leaf-mates over all leaves listed (leaf l = pts[ptr[l] .. ptr[l+1])) and its incoming
+ * heap row Din/Iin (ids found in a leaf take the leaf's distance). Output sorted ascending. */
+void oracle_allnn_leaves_s(int N, int d, int k, const float *X, const float *X2, int nleaves,
+                           const int *ptr, const int *pts, const float *Din, const int *Iin,
+                           int ldin, double *Dout, int *Iout);
+
 /* Heap checks: 1 if every row is a valid binary (or 4-ary with header) max-heap. */
 int oracle_is_maxheap_d(int n, int k, int ld, const double *D);
 int oracle_is_maxheap_s(int n, int k, int ld, const float *D);

@@ -109,6 +109,20 @@ class Oracle:
                                       _p(Din), _p(Iin), _i(ldin), _p(Dout), _p(Iout))
         return Dout, Iout
 
+    def allnn_leaves(self, k, X, X2, ptr, pts, Din=None, Iin=None):
+        """Batching form: per point, the k nearest among its leaf-mates (all leaves given)
+        and its incoming heap row; FP64, sorted ascending, lower id first on ties."""
+        N, d = X.shape
+        Dout = np.empty((N, k), dtype=np.float64)
+        Iout = np.empty((N, k), dtype=np.int32)
+        ptr = np.ascontiguousarray(ptr, dtype=np.int32)
+        pts = np.ascontiguousarray(pts, dtype=np.int32)
+        ldin = 0 if Din is None else Din.shape[1]
+        self.lib.oracle_allnn_leaves_s(_i(N), _i(d), _i(k), _p(X), _p(X2), _i(ptr.size - 1),
+                                       _p(ptr), _p(pts), _p(Din), _p(Iin), _i(ldin), _p(Dout),
+                                       _p(Iout))
+        return Dout, Iout
+
     def is_maxheap(self, D, k=None):
         n, ld = D.shape
         k = ld if k is None else k

@@ -17,6 +17,10 @@
 
 namespace gsknn {
 
+// Sets the calling thread's status (read by gsknn_last_error / gsknn_last_error_string) and
+// returns `code`; fmt == nullptr means "ok".
+int set_status(int code, const char *fmt, ...);
+
 struct SimtGeom {
   int kp;      // list length (power of two >= k, >= 32), 0 when k is unsupported
   int bq, br;  // queries / candidates per CTA tile

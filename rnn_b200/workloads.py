@@ -173,3 +173,40 @@ def config3(seed: int = 3, n_queries: int = 32768, n_refs: int = 262144, d: int 
     alpha = perm[n_queries:]
     return KnnProblem(X, sq_norms(X), alpha, beta, k,
                       f"precision f32 d={d} queries={n_queries} refs={n_refs} k={k}")
+
+
+class AllNnProblem:
+    """All-nearest-neighbour search over randomized-tree leaves (the batching form)."""
+
+    def __init__(self, X, X2, k, trees_per_pass, passes, leaf_min, leaf_max, tree_seed, name=""):
+        self.X = X
+        self.X2 = X2
+        self.k = int(k)
+        self.trees_per_pass = int(trees_per_pass)
+        self.passes = int(passes)
+        self.leaf_min = int(leaf_min)
+        self.leaf_max = int(leaf_max)
+        self.tree_seed = int(tree_seed)
+        self.name = name
+
+    @property
+    def N(self):
+        return self.X.shape[0]
+
+    @property
+    def d(self):
+        return self.X.shape[1]
+
+
+def config4(seed: int = 4, n_points: int = 1 << 21, d: int = 64, k: int = 32,
+            trees_per_pass: int = 8, passes: int = 4, leaf_min: int = 256,
+            leaf_max: int = 2048):
+    """Batching form: N=2,097,152 float32 points of a 16-Gaussian mixture (sigma 0.05), d=64;
+    8 randomized trees per pass, leaf sizes uniform in [256, 2048], alpha = beta = leaf, k=32,
+    heaps merged over 4 passes."""
+    X = gaussian_mixture_table(seed, n_points, d, dtype=np.float32)
+    return AllNnProblem(X, sq_norms(X), k, trees_per_pass, passes, leaf_min, leaf_max,
+                        seed + 500,
+                        f"all-NN over rkd-tree leaves: N={n_points} d={d} k={k} "
+                        f"{trees_per_pass} trees/pass x {passes} passes, "
+                        f"leaves U[{leaf_min},{leaf_max}]")
