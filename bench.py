@@ -24,6 +24,11 @@ seeded; the reference publishes no dataset for this path.
            points, alpha = beta = leaf, 4 passes merged into one heap): every leaf of a pass in
            one persistent launch replayed from a CUDA graph, tile shape by the autotuner;
            distance evaluations (sum of leaf sizes squared) per second over the 4 passes.
+`serving_form`: requests against a resident reference set (4,194,304 points, d = 128,
+           U[0,1)): Poisson arrivals, m log-uniform in [1, 4096] queries, k from {8, 16, 64};
+           continuous batching inside the library; p50 / p99 latency (submit to result on the
+           device) and aggregate distance evaluations/s, beside the same requests run one by
+           one through the plain FP32 kernel and through the per-call tensor-core path.
 `roofline`: the dominant kernel of the headline run; contraction counted as 2d flops per
            evaluation, against the measured bf16 dense peak (MEASURED_PEAKS.json; half of it
            for TF32, the TF32 tensor rate) or, for the CUDA-core kernel, the FP32 issue rate at
@@ -82,6 +87,14 @@ def parse():
     ap.add_argument("--batch-points", type=int, default=1 << 21,
                     help="points of the batching-form workload (smaller for profiling)")
     ap.add_argument("--batch-passes", type=int, default=4)
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-form workload")
+    ap.add_argument("--serve-only", action="store_true",
+                    help="only the serving-form workload (Poisson requests, resident set)")
+    ap.add_argument("--serve-refs", type=int, default=1 << 22,
+                    help="resident reference points of the serving workload")
+    ap.add_argument("--serve-requests", type=int, default=400)
+    ap.add_argument("--serve-rate", type=float, default=150.0,
+                    help="mean request arrival rate (requests/s, Poisson)")
     ap.add_argument("--cpu-worker", default=None, help=argparse.SUPPRESS)
     return ap.parse_args()
 
@@ -384,6 +397,8 @@ def run_ours(args, rank, world, local_rank):
     out = {}
     if args.batch_only:
         return batching_form(L, G, W, dev, peaks, args, args.threads)
+    if args.serve_only:
+        return serving_form(L, G, W, dev, args)
     if not args.precision_only:
         p = W.config2(seed=2)
         nq = args.queries
@@ -442,6 +457,8 @@ def run_ours(args, rank, world, local_rank):
         out["precision_form"] = pf
         if not args.no_batch and not args.profile_only:
             out["batching_form"] = batching_form(L, G, W, dev, peaks, args, args.threads)
+        if not args.no_serve and not args.profile_only:
+            out["serving_form"] = serving_form(L, G, W, dev, args)
     G.set_mode(0)
     return out
 
@@ -551,6 +568,117 @@ def batching_form(L, G, W, dev, peaks, args, threads):
     return res
 
 
+def serving_form(L, G, W, dev, args):
+    """Poisson request stream against a resident reference set (continuous batching)."""
+    import threading
+    import torch
+    from rnn_b200 import serve as SV
+    nref, d = args.serve_refs, 128
+    R = W.uniform_table(5, nref, d).astype(np.float32)
+    R2 = W.sq_norms(R)
+    Rd = torch.from_numpy(R).to(dev)
+    R2d = torch.from_numpy(R2).to(dev)
+    del R
+    rng = np.random.default_rng(55)
+    n = args.serve_requests
+    ms = np.floor(np.exp(rng.uniform(0.0, np.log(4096.0), size=n))).astype(int).clip(1, 4096)
+    ks = rng.choice([8, 16, 64], size=n)
+    gaps = rng.exponential(1.0 / args.serve_rate, size=n)
+    qs = [W.uniform_table(5000 + i, int(ms[i]), d).astype(np.float32) for i in range(n)]
+    srv = SV.Server(Rd, R2d, mode=0, max_batch_queries=8192, max_k=64, heap_budget=2 << 30,
+                    slots=3)
+    for m_w in (1, 128, 4096):  # warm-up: module loads, first launches of every kernel
+        rid = srv.submit(W.uniform_table(99, m_w, d).astype(np.float32), 64)
+        srv.wait(rid)
+        srv.release(rid)
+    ids = [None] * n
+    submitted = threading.Event()
+
+    def arrivals():
+        t = time.perf_counter()
+        for i in range(n):
+            t += gaps[i]
+            dt = t - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            ids[i] = srv.submit(qs[i], int(ks[i]))
+        submitted.set()
+
+    lat, queue, rows = [], [], []
+    t0 = time.perf_counter()
+    th = threading.Thread(target=arrivals)
+    th.start()
+    for i in range(n):
+        while ids[i] is None:
+            time.sleep(0.0002)
+        srv.wait(ids[i], timeout=120.0)
+        st = srv.stats(ids[i])
+        lat.append(st["total_ms"])
+        queue.append(st["queue_ms"])
+        rows.append(st["batch_rows"])
+        srv.release(ids[i])
+    t1 = time.perf_counter()
+    th.join()
+    srv.close()
+    evals = float(ms.sum()) * nref
+    lat = np.asarray(lat)
+    big = lat[ms >= 2048]
+    res = {
+        "workload": (f"serving: resident refs={nref} d={d} U[0,1); {n} requests, Poisson "
+                     f"{args.serve_rate:g}/s, m log-uniform [1,4096] (mean {ms.mean():.0f}), "
+                     f"k in {{8,16,64}}"),
+        "dtype": "f32 inputs; tf32 tensor distances + fp64 re-rank (exact top-k)",
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "max": float(lat.max()),
+                       "p50_m_ge_2048": float(np.percentile(big, 50)) if big.size else None,
+                       "p99_m_ge_2048": float(np.percentile(big, 99)) if big.size else None,
+                       "queue_p50": float(np.percentile(queue, 50)),
+                       "queue_p99": float(np.percentile(queue, 99))},
+        "value": evals / (t1 - t0), "unit": "distance-evals/s",
+        "wall_s": t1 - t0, "mean_batch_rows": float(np.mean(rows)),
+        "p99_target_ms": 5.0,
+    }
+    # the same requests one at a time through the per-call entry point: plain FP32 CUDA-core
+    # kernel and the per-call tensor-core path (which re-packs the reference set each call)
+    sample = list(range(0, n, max(1, n // 24)))
+    alpha = torch.arange(nref, dtype=torch.int32, device=dev)
+    for name, mode in (("per_request_fp32", 1), ("per_request_tc", 0)):
+        G.set_mode(mode)
+        tot_e, tot_ms, lats = 0.0, 0.0, []
+        for i in sample:
+            Q = torch.from_numpy(qs[i]).to(dev)
+            Q2 = torch.from_numpy(W.sq_norms(qs[i])).to(dev)
+            beta = torch.arange(int(ms[i]), dtype=torch.int32, device=dev)
+            k = int(ks[i])
+            D = torch.full((int(ms[i]), k), float("inf"), device=dev)
+            I = torch.full((int(ms[i]), k), -1, dtype=torch.int32, device=dev)
+            st = torch.cuda.current_stream(dev)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            rc = L.gsknn_s_device(nref, int(ms[i]), d, k, Rd.data_ptr(), R2d.data_ptr(), nref,
+                                  alpha.data_ptr(), Q.data_ptr(), Q2.data_ptr(), int(ms[i]),
+                                  beta.data_ptr(), D.data_ptr(), I.data_ptr(), k,
+                                  st.cuda_stream)
+            e1.record(st)
+            torch.cuda.synchronize()
+            if rc != 0:
+                raise RuntimeError(G.last_error())
+            t = e0.elapsed_time(e1)
+            lats.append(t)
+            tot_ms += t
+            tot_e += float(ms[i]) * nref
+        res[name] = {"requests": len(sample), "value": tot_e / (tot_ms * 1e-3),
+                     "latency_ms_p50": float(np.percentile(lats, 50)),
+                     "latency_ms_max": float(np.max(lats))}
+    G.set_mode(0)
+    res["speedup_vs_per_request_fp32"] = res["value"] / res["per_request_fp32"]["value"]
+    del Rd, R2d
+    torch.cuda.empty_cache()
+    return res
+
+
 def e2e_host(L, G, p, beta_h, args):
     import ctypes
     import torch
@@ -623,7 +751,7 @@ def main():
     args.threads = threads
     out = run_ours(args, rank, world, local_rank)
     if (rank == 0 and world == 1 and not args.no_cpu_baseline and not args.profile_only
-            and not args.precision_only and not args.batch_only):
+            and not args.precision_only and not args.batch_only and not args.serve_only):
         try:
             out["cpu_baseline"] = cpu_baseline(args.cpu_seconds, threads)
         except Exception as e:  # reported, not fatal

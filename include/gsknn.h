@@ -260,6 +260,44 @@ void gsknn_batch_destroy(gsknn_batch_t *job);
 /* Forgets every tile shape the autotuner has chosen in this process. */
 void gsknn_batch_forget_tuning(void);
 
+/* ---- Serving form: requests against a device-resident reference set -----------------------
+ * No counterpart in the reference (a caller would run sgsknn once per request).
+ *
+ * gsknn_serve_create prepares the nref x d float reference set R (device pointer, with norms
+ * R2) once: packed for the tensor cores (mode AUTO / TF32 / BF16 / BF16X3; AUTO = split BF16
+ * below d = 128, TF32 from there) and resident until destroy. Each request is m query rows
+ * (host memory, copied at submit) and a k <= max_k; its result is the exact FP64 top-k of every
+ * query against R (ties to the lower id), as a heap of m rows x k (descending rows) that stays
+ * on the device until the request is released.
+ *
+ * A dispatcher thread admits queued requests in arrival order while their heaps (m*k*8 bytes)
+ * fit `heap_budget` bytes of device memory, packs admitted requests into batches of at most
+ * max_batch_queries rows and runs each batch on one of `slots` streams: requests that arrive
+ * while a batch is on the GPU start in the next free slot (continuous batching). A request's
+ * result does not depend on its batch. Released requests return their heap memory to the
+ * budget; requests that are never released keep it, and later requests then wait. */
+typedef struct gsknn_serve_s gsknn_serve_t;
+gsknn_serve_t *gsknn_serve_create(const float *R, const float *R2, int nref, int d, int mode,
+                                  int max_batch_queries, int max_k, size_t heap_budget,
+                                  int slots);
+/* Returns the request id (>= 0), or minus an error code. */
+long long gsknn_serve_submit(gsknn_serve_t *eng, const float *Q, int m, int k);
+/* 1 done, 0 pending, negative: unknown request or failed. */
+int gsknn_serve_test(gsknn_serve_t *eng, long long id);
+int gsknn_serve_wait(gsknn_serve_t *eng, long long id, double timeout_s);
+/* Device pointers of a finished request's heap (m x k floats, m x k ints). */
+int gsknn_serve_heap(gsknn_serve_t *eng, long long id, float **D, int **I);
+/* Copies a finished request's heap to host memory. */
+int gsknn_serve_fetch(gsknn_serve_t *eng, long long id, float *D, int *I);
+/* Milliseconds from submit to launch and from submit to completion; batch number and rows. */
+int gsknn_serve_stats(gsknn_serve_t *eng, long long id, double *queue_ms, double *total_ms,
+                      int *batch, int *batch_rows);
+int gsknn_serve_release(gsknn_serve_t *eng, long long id);
+/* While paused (nonzero) the dispatcher starts no new batch; requests still queue. Running
+ * batches finish. Resuming dispatches everything queued in arrival order. */
+int gsknn_serve_pause(gsknn_serve_t *eng, int paused);
+void gsknn_serve_destroy(gsknn_serve_t *eng);
+
 /* Randomized projection trees on the host (the caller side of the batching form): `ntrees`
  * trees over the N x d row-major float points X. Each tree first draws leaf sizes uniformly in
  * [leaf_min, leaf_max] (leaf_max >= 2 leaf_min) that sum to N, then splits every node along a

@@ -103,17 +103,53 @@ struct TcPlan {
   int N, NST, qtiles, rtiles, q_pad, r_pad, S, tiles_per_split, logcap;
   unsigned smem;
   float coefA, coefB;
-  size_t o_mu, o_mu2, o_stats, o_pa, o_pa_lo, o_pb, o_pb_lo, o_qn, o_qnrm, o_cn, o_cnrm,
-      o_cid, o_log, o_logcnt, o_kth, o_kth_shared, o_margin, o_fbl, o_fbc;
-  size_t bytes;
+  // query-side workspace offsets (absolute within the workspace; they start after the
+  // prepared-candidate area when the plan includes it)
+  size_t o_pa, o_pa_lo, o_qn, o_qnrm, o_log, o_logcnt, o_kth, o_kth_shared, o_margin, o_fbl,
+      o_fbc;
+  size_t cand_bytes;  // prepared-candidate area at the start of the workspace (0: separate)
+  size_t bytes;       // whole workspace
 };
 
-TcPlan tc_plan(int nq, int nc, int d, int k, int mode, int sms);
+// Candidates packed once in the MMA input format, with everything a query batch needs from
+// them: shift mu, |mu|^2, bound statistics (max centred norm, max |effective norm|), packed
+// panels [r_pad][d_pad] (r_pad a multiple of 256), effective norms, centred norm bounds, ids,
+// and the caller's table for the FP64 re-rank. A resident reference set is prepared once and
+// serves any number of query batches.
+struct TcCand {
+  int fmt, elem, d, d_pad, nc, r_pad;
+  float *mu;
+  double *mu2;
+  unsigned *stats;
+  void *pb, *pb_lo;
+  float *cn, *cnrm;
+  uint32_t *cid;
+  const float *Xc, *Xc2;
+  long long nrows_c;
+  const int *cidx;
+};
+
+int tc_format_of_mode(int mode);
+size_t tc_cand_bytes(int nc, int d, int mode);
+cudaError_t tc_cand_prepare(TcCand *C, void *mem, int nc, int d, int mode, const float *Xc,
+                            const float *Xc2, long long nrows_c, const int *cidx, int *status,
+                            cudaStream_t st);
+
+// with_cand: the workspace starts with the prepared-candidate area (tc_run); otherwise the
+// plan covers the query side only (tc_run_prepared with separately prepared candidates).
+// max_splits caps the candidate splits per query tile (0: the default, 16).
+TcPlan tc_plan(int nq, int nc, int d, int k, int mode, int sms, bool with_cand = true,
+               int max_splits = 0);
 cudaError_t tc_run(const TcPlan &P, int nq, int nc, int d, int k, const float *Xq,
                    const float *Xq2, long long nrows_q, const int *qidx, const float *Xc,
                    const float *Xc2, long long nrows_c, const int *cidx, float *D, int *I,
                    int ldD, void *ws, int *status, float *dbg, long long dbg_ld,
                    unsigned long long *counters, cudaStream_t st, TraceHook hook,
                    void *hook_ctx);
+cudaError_t tc_run_prepared(const TcPlan &P, const TcCand &C, int nq, int d, int k,
+                            const float *Xq, const float *Xq2, long long nrows_q,
+                            const int *qidx, float *D, int *I, int ldD, void *ws, int *status,
+                            float *dbg, long long dbg_ld, unsigned long long *counters,
+                            cudaStream_t st, TraceHook hook, void *hook_ctx);
 
 }  // namespace gsknn

@@ -954,7 +954,65 @@ int tc_format_of_mode(int mode) {
   return mode == GSKNN_TC_BF16 ? 1 : mode == GSKNN_TC_BF16X3 ? 2 : 0;
 }
 
-TcPlan tc_plan(int nq, int nc, int d, int k, int mode, int sms) {
+// Prepared-candidate area: mu, mu2, stats, panel(s), norms, norm bounds, ids.
+struct CandLayout {
+  size_t o_mu, o_mu2, o_stats, o_pb, o_pb_lo, o_cn, o_cnrm, o_cid, bytes;
+  int fmt, elem, d_pad, r_pad;
+};
+
+static CandLayout cand_layout(int nc, int d, int mode) {
+  using namespace tc;
+  CandLayout L{};
+  L.fmt = tc_format_of_mode(mode);
+  L.elem = L.fmt == 0 ? 4 : 2;
+  const int celems = CHUNK_BYTES / L.elem;
+  L.d_pad = ((d + celems - 1) / celems) * celems;
+  L.r_pad = ((nc + 255) / 256) * 256;  // whole tiles of 256 and of 128 candidates
+  size_t off = 0;
+  auto take = [&](size_t b) { size_t o = off; off = al256(off + b); return o; };
+  L.o_mu = take((size_t)d * 4);
+  L.o_mu2 = take(8);
+  L.o_stats = take(16);
+  L.o_pb = take((size_t)L.r_pad * L.d_pad * L.elem);
+  L.o_pb_lo = L.fmt == 2 ? take((size_t)L.r_pad * L.d_pad * L.elem) : 0;
+  L.o_cn = take((size_t)L.r_pad * 4);
+  L.o_cnrm = take((size_t)L.r_pad * 4);
+  L.o_cid = take((size_t)L.r_pad * 4);
+  L.bytes = off;
+  return L;
+}
+
+size_t tc_cand_bytes(int nc, int d, int mode) { return cand_layout(nc, d, mode).bytes; }
+
+cudaError_t tc_cand_prepare(TcCand *C, void *mem, int nc, int d, int mode, const float *Xc,
+                            const float *Xc2, long long nrows_c, const int *cidx, int *status,
+                            cudaStream_t st) {
+  using namespace tc;
+  const CandLayout L = cand_layout(nc, d, mode);
+  char *base = static_cast<char *>(mem);
+  C->fmt = L.fmt; C->elem = L.elem; C->d = d; C->d_pad = L.d_pad; C->nc = nc; C->r_pad = L.r_pad;
+  C->mu = reinterpret_cast<float *>(base + L.o_mu);
+  C->mu2 = reinterpret_cast<double *>(base + L.o_mu2);
+  C->stats = reinterpret_cast<unsigned *>(base + L.o_stats);
+  C->pb = base + L.o_pb;
+  C->pb_lo = L.fmt == 2 ? base + L.o_pb_lo : nullptr;
+  C->cn = reinterpret_cast<float *>(base + L.o_cn);
+  C->cnrm = reinterpret_cast<float *>(base + L.o_cnrm);
+  C->cid = reinterpret_cast<uint32_t *>(base + L.o_cid);
+  C->Xc = Xc; C->Xc2 = Xc2; C->nrows_c = nrows_c; C->cidx = cidx;
+  cudaError_t e = cudaMemsetAsync(C->stats, 0, 16, st);
+  if (e != cudaSuccess) return e;
+  const int nsample = std::min(nc, 4096);
+  tc_center<<<(d + 31) / 32, 1024, 0, st>>>(Xc, d, nrows_c, cidx, nc, nsample, C->mu);
+  tc_mu2<<<1, 32, 0, st>>>(C->mu, d, C->mu2);
+  tc_pack<<<(L.r_pad + 7) / 8, 256, 0, st>>>(L.fmt, Xc, Xc2, d, L.d_pad, nrows_c, cidx, nc,
+                                            L.r_pad, C->mu, C->mu2, 1, C->pb, C->pb_lo, C->cn,
+                                            C->cnrm, C->cid, C->stats, status);
+  return cudaGetLastError();
+}
+
+TcPlan tc_plan(int nq, int nc, int d, int k, int mode, int sms, bool with_cand,
+               int max_splits) {
   using namespace tc;
   TcPlan P{};
   P.ok = false;
@@ -985,13 +1043,14 @@ TcPlan tc_plan(int nq, int nc, int d, int k, int mode, int sms) {
   P.NST = best_NST;
   P.smem = tc_smem_layout(P.nkc, P.a_terms, P.b_terms, P.N, P.NST, k).total;
   P.qtiles = (nq + TC_M - 1) / TC_M;
-  P.rtiles = (nc + P.N - 1) / P.N;
+  P.r_pad = ((nc + 255) / 256) * 256;
+  P.rtiles = P.r_pad / P.N;
   P.q_pad = P.qtiles * TC_M;
-  P.r_pad = P.rtiles * P.N;
   // splits: balance waves (one CTA per SM)
+  const int smax = std::min(P.rtiles, max_splits > 0 ? max_splits : 16);
   int best_s = 1;
   double best = 1e300;
-  for (int s = 1; s <= std::min(P.rtiles, 16); s++) {
+  for (int s = 1; s <= smax; s++) {
     const long long items = (long long)P.qtiles * s;
     // each split pays a start-up burst before the shared threshold tightens
     const double cost = (double)((items + sms - 1) / sms) / s * (1.0 + 0.03 * s);
@@ -1000,21 +1059,14 @@ TcPlan tc_plan(int nq, int nc, int d, int k, int mode, int sms) {
   P.S = best_s;
   P.tiles_per_split = (P.rtiles + P.S - 1) / P.S;
   P.logcap = std::max(8 * P.kp, 1024);
-  // workspace
-  size_t off = 0;
+  // workspace: [prepared candidates | query side]
+  P.cand_bytes = with_cand ? al256(tc_cand_bytes(nc, d, mode)) : 0;
+  size_t off = P.cand_bytes;
   auto take = [&](size_t b) { size_t o = off; off = al256(off + b); return o; };
-  P.o_mu = take((size_t)d * 4);
-  P.o_mu2 = take(8);
-  P.o_stats = take(16);
   P.o_pa = take((size_t)P.q_pad * P.d_pad * elem);
   P.o_pa_lo = P.fmt == 2 ? take((size_t)P.q_pad * P.d_pad * elem) : 0;
-  P.o_pb = take((size_t)P.r_pad * P.d_pad * elem);
-  P.o_pb_lo = P.fmt == 2 ? take((size_t)P.r_pad * P.d_pad * elem) : 0;
   P.o_qn = take((size_t)P.q_pad * 4);
   P.o_qnrm = take((size_t)P.q_pad * 4);
-  P.o_cn = take((size_t)P.r_pad * 4);
-  P.o_cnrm = take((size_t)P.r_pad * 4);
-  P.o_cid = take((size_t)P.r_pad * 4);
   // two logs per (query, split): one per epilogue warp of a lane quarter
   P.o_log = take((size_t)2 * P.S * nq * P.logcap * 8);
   P.o_logcnt = take((size_t)2 * P.S * nq * 4);
@@ -1048,24 +1100,33 @@ cudaError_t tc_run(const TcPlan &P, int nq, int nc, int d, int k, const float *X
                    int ldD, void *ws, int *status, float *dbg, long long dbg_ld,
                    unsigned long long *counters, cudaStream_t st, TraceHook hook,
                    void *hook_ctx) {
+  if (P.cand_bytes == 0) return cudaErrorInvalidValue;
+  // centre, mu.mu and the candidate pack share the tracer's packing bracket
+  if (hook) hook(hook_ctx, "tc_pack", true, st, 0);
+  TcCand C{};
+  const int mode = P.fmt == 1 ? GSKNN_TC_BF16 : P.fmt == 2 ? GSKNN_TC_BF16X3 : GSKNN_TC_TF32;
+  cudaError_t e = tc_cand_prepare(&C, ws, nc, d, mode, Xc, Xc2, nrows_c, cidx, status, st);
+  if (hook) hook(hook_ctx, "tc_pack", false, st, 3);
+  if (e != cudaSuccess) return e;
+  return tc_run_prepared(P, C, nq, d, k, Xq, Xq2, nrows_q, qidx, D, I, ldD, ws, status, dbg,
+                         dbg_ld, counters, st, hook, hook_ctx);
+}
+
+cudaError_t tc_run_prepared(const TcPlan &P, const TcCand &C, int nq, int d, int k,
+                            const float *Xq, const float *Xq2, long long nrows_q,
+                            const int *qidx, float *D, int *I, int ldD, void *ws, int *status,
+                            float *dbg, long long dbg_ld, unsigned long long *counters,
+                            cudaStream_t st, TraceHook hook, void *hook_ctx) {
   using namespace tc;
+  if (C.fmt != P.fmt || C.d_pad != P.d_pad || C.r_pad != P.r_pad) return cudaErrorInvalidValue;
   char *base = static_cast<char *>(ws);
-  float *mu = reinterpret_cast<float *>(base + P.o_mu);
-  double *mu2 = reinterpret_cast<double *>(base + P.o_mu2);
-  unsigned *stats = reinterpret_cast<unsigned *>(base + P.o_stats);
   void *pa = base + P.o_pa;
   void *pa_lo = P.fmt == 2 ? base + P.o_pa_lo : nullptr;
-  void *pb = base + P.o_pb;
-  void *pb_lo = P.fmt == 2 ? base + P.o_pb_lo : nullptr;
   float *qn = reinterpret_cast<float *>(base + P.o_qn);
   float *qnrm = reinterpret_cast<float *>(base + P.o_qnrm);
-  float *cn = reinterpret_cast<float *>(base + P.o_cn);
-  float *cnrm = reinterpret_cast<float *>(base + P.o_cnrm);
-  uint32_t *cid = reinterpret_cast<uint32_t *>(base + P.o_cid);
   int *fbc = reinterpret_cast<int *>(base + P.o_fbc);
-  cudaError_t e;
-  e = cudaMemsetAsync(stats, 0, 16, st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(fbc, 0, 16, st);
+  const int nc = C.nc;
+  cudaError_t e = cudaMemsetAsync(fbc, 0, 16, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(base + P.o_kth_shared, 0xFF, (size_t)nq * 4, st);
   if (e != cudaSuccess) return e;
 
@@ -1074,28 +1135,22 @@ cudaError_t tc_run(const TcPlan &P, int nq, int nc, int d, int k, const float *X
     if (hook) hook(hook_ctx, name, begin, st, nk);
   };
   mark("tc_pack", true);
-  const int nsample = std::min(nc, 4096);
-  tc_center<<<(d + 31) / 32, 1024, 0, st>>>(Xc, d, nrows_c, cidx, nc, nsample, mu);
-  tc_mu2<<<1, 32, 0, st>>>(mu, d, mu2);
-  tc_pack<<<(P.r_pad + 7) / 8, 256, 0, st>>>(P.fmt, Xc, Xc2, d, P.d_pad, nrows_c, cidx, nc,
-                                            P.r_pad, mu, mu2, 1, pb, pb_lo, cn, cnrm, cid,
-                                            stats, status);
   tc_pack<<<(P.q_pad + 7) / 8, 256, 0, st>>>(P.fmt, Xq, Xq2, d, P.d_pad, nrows_q, qidx, nq,
-                                            P.q_pad, mu, mu2, 0, pa, pa_lo, qn, qnrm, nullptr,
-                                            stats, status);
+                                            P.q_pad, C.mu, C.mu2, 0, pa, pa_lo, qn, qnrm,
+                                            nullptr, C.stats, status);
   e = cudaGetLastError();
-  mark("tc_pack", false, 4);  // centre, mu.mu, two packs
+  mark("tc_pack", false, 1);  // query pack
   if (e != cudaSuccess) return e;
 
   CUtensorMap mA, mAlo, mB, mBlo;
   e = make_panel_map(&mA, pa, P.elem, P.d_pad, P.q_pad, TC_M);
-  if (e == cudaSuccess) e = make_panel_map(&mB, pb, P.elem, P.d_pad, P.r_pad, P.N);
+  if (e == cudaSuccess) e = make_panel_map(&mB, C.pb, P.elem, P.d_pad, P.r_pad, P.N);
   if (e != cudaSuccess) return e;
   mAlo = mA;
   mBlo = mB;
   if (P.fmt == 2) {
     e = make_panel_map(&mAlo, pa_lo, P.elem, P.d_pad, P.q_pad, TC_M);
-    if (e == cudaSuccess) e = make_panel_map(&mBlo, pb_lo, P.elem, P.d_pad, P.r_pad, P.N);
+    if (e == cudaSuccess) e = make_panel_map(&mBlo, C.pb_lo, P.elem, P.d_pad, P.r_pad, P.N);
     if (e != cudaSuccess) return e;
   }
   TcParams tp{};
@@ -1103,7 +1158,7 @@ cudaError_t tc_run(const TcPlan &P, int nq, int nc, int d, int k, const float *X
   tp.tiles_per_split = P.tiles_per_split; tp.N = P.N; tp.NST = P.NST; tp.logcap = P.logcap;
   tp.a_terms = P.a_terms; tp.b_terms = P.b_terms; tp.fmt = P.fmt;
   tp.idesc = idesc_f32acc(P.fmt == 0 ? 2u : 1u, TC_M, P.N);
-  tp.cn = cn; tp.cid = cid; tp.qn = qn; tp.qnrm = qnrm; tp.stats = stats;
+  tp.cn = C.cn; tp.cid = C.cid; tp.qn = qn; tp.qnrm = qnrm; tp.stats = C.stats;
   tp.Din = D; tp.ldD = ldD; tp.coefA = P.coefA; tp.coefB = P.coefB;
   tp.log = reinterpret_cast<uint2 *>(base + P.o_log);
   tp.logcnt = reinterpret_cast<int *>(base + P.o_logcnt);
@@ -1135,14 +1190,14 @@ cudaError_t tc_run(const TcPlan &P, int nq, int nc, int d, int k, const float *X
   rp.Q = nq; rp.k = k; rp.S = 2 * P.S; rp.logcap = P.logcap; rp.d = d;
   rp.log = tp.log; rp.logcnt = tp.logcnt; rp.kth = tp.kth; rp.margin = tp.margin;
   rp.kth_shared = tp.kth_shared;
-  rp.Xq = Xq; rp.Xq2 = Xq2; rp.Xc = Xc; rp.Xc2 = Xc2; rp.qidx = qidx; rp.cid = cid;
+  rp.Xq = Xq; rp.Xq2 = Xq2; rp.Xc = C.Xc; rp.Xc2 = C.Xc2; rp.qidx = qidx; rp.cid = C.cid;
   rp.D = D; rp.I = I; rp.ldD = ldD;
   rp.fallback_list = reinterpret_cast<int *>(base + P.o_fbl);
   rp.fallback_count = fbc;
   rp.counters = counters;
   FallbackParams fp{};
-  fp.k = k; fp.d = d; fp.nc = nc; fp.Xq = Xq; fp.Xq2 = Xq2; fp.Xc = Xc; fp.Xc2 = Xc2;
-  fp.qidx = qidx; fp.cidx = cidx; fp.nrows_c = nrows_c; fp.D = D; fp.I = I; fp.ldD = ldD;
+  fp.k = k; fp.d = d; fp.nc = nc; fp.Xq = Xq; fp.Xq2 = Xq2; fp.Xc = C.Xc; fp.Xc2 = C.Xc2;
+  fp.qidx = qidx; fp.cidx = C.cidx; fp.nrows_c = C.nrows_c; fp.D = D; fp.I = I; fp.ldD = ldD;
   fp.list = rp.fallback_list; fp.count = fbc;
   const int rb = (nq + 7) / 8;
   mark("tc_rerank", true);
