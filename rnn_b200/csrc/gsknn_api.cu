@@ -18,6 +18,7 @@
 #include <string>
 #include <tuple>
 #include <type_traits>
+#include <thread>
 #include <vector>
 
 namespace gsknn {
@@ -54,7 +55,7 @@ int set_status(int code, const char *fmt, ...) {
 // scratch cache
 // ------------------------------------------------------------------------------------------
 enum Slot { SLOT_KERNEL = 0, SLOT_STATUS, SLOT_HQTAB, SLOT_HCTAB, SLOT_HQNRM, SLOT_HCNRM,
-            SLOT_HQIDX, SLOT_HCIDX, SLOT_HD, SLOT_HI, SLOT_AUX };
+            SLOT_HQIDX, SLOT_HCIDX, SLOT_HD, SLOT_HI, SLOT_AUX, SLOT_HGATHER };
 
 struct Buf {
   void *p = nullptr;
@@ -145,6 +146,68 @@ struct TraceScope {
     g_recs.push_back({name, a, b, nk});
   }
 };
+
+// Pinned host staging of the calling thread (the gathered rows of a host call), kept between
+// calls and freed when the thread exits.
+struct PinnedStage {
+  void *p = nullptr;
+  size_t n = 0;
+  ~PinnedStage() {
+    if (p) cudaFreeHost(p);
+  }
+};
+static thread_local PinnedStage t_stage;
+
+static cudaError_t pinned_stage(size_t bytes, void **out) {
+  if (t_stage.n < bytes) {
+    if (t_stage.p) cudaFreeHost(t_stage.p);
+    t_stage.p = nullptr;
+    t_stage.n = 0;
+    cudaError_t e = cudaHostAlloc(&t_stage.p, bytes, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      return e;
+    }
+    t_stage.n = bytes;
+  }
+  *out = t_stage.p;
+  return cudaSuccess;
+}
+
+// Rows idx[0..n) of the row-major table X (d per row) and their norms, copied one after another
+// into dst / dst2 by parallel host threads.
+template <typename T>
+static void gather_rows(const T *X, const T *X2, int d, const int *idx, int n, T *dst, T *dst2) {
+  unsigned nt = std::thread::hardware_concurrency();
+  if (nt == 0) nt = 1;
+  if (nt > 32) nt = 32;
+  const size_t bytes = (size_t)n * d * sizeof(T);
+  if (bytes < ((size_t)8 << 20)) nt = 1;
+  auto work = [&](unsigned w) {
+    const int a = (int)((long long)n * w / nt), b = (int)((long long)n * (w + 1) / nt);
+    for (int i = a; i < b; i++) {
+      std::memcpy(dst + (size_t)i * d, X + (size_t)idx[i] * d, (size_t)d * sizeof(T));
+      dst2[i] = X2[idx[i]];
+    }
+  };
+  std::vector<std::thread> pool;
+  for (unsigned w = 1; w < nt; w++) pool.emplace_back(work, w);
+  work(0);
+  for (auto &t : pool) t.join();
+}
+
+// table[(idx[i] - lo)] = rows[i] (and the norms), one warp per row
+template <typename T>
+__global__ void scatter_rows(const T *__restrict__ rows, const T *__restrict__ rows2,
+                             const int *__restrict__ idx, int n, int d, int lo, T *__restrict__ tab,
+                             T *__restrict__ tab2) {
+  const int lane = threadIdx.x & 31;
+  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (i >= n) return;
+  const size_t r = (size_t)(idx[i] - lo);
+  for (int p = lane; p < d; p += 32) tab[r * d + p] = rows[(size_t)i * d + p];
+  if (lane == 0) tab2[r] = rows2[i];
+}
 
 static cudaStream_t host_stream() {
   static thread_local std::map<int, cudaStream_t> streams;
@@ -314,27 +377,31 @@ static int knn_device_tc(int mode, int nq, int nc, int d, int k, const float *Xq
   unsigned long long *counters = nullptr;
   if (want_counters) {
     void *cv = nullptr;
-    CU(scratch(SLOT_AUX, 64, st, &cv));
+    CU(scratch(SLOT_AUX, 128, st, &cv));
     counters = static_cast<unsigned long long *>(cv);
-    CU(cudaMemsetAsync(counters, 0, 64, st));
+    CU(cudaMemsetAsync(counters, 0, 128, st));
   }
   CU(tc_run(P, nq, nc, d, k, Xq, Xq2, nrows_q, qidx, Xc, Xc2, nrows_c, cidx, D, I, ldD, ws,
             status, dbg, dbg_ld, counters, st, trace_hook, nullptr));
   if (counters) {
-    unsigned long long h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    unsigned long long h[16] = {};
     int nfb = 0;
     CU(cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, st));
     CU(cudaMemcpyAsync(&nfb, static_cast<char *>(ws) + P.o_fbc, sizeof(int),
                        cudaMemcpyDeviceToHost, st));
     CU(cudaStreamSynchronize(st));
+    const double ctas = (double)P.qtiles * P.S, warps = ctas * 8.0;
     std::fprintf(stderr,
-                 "gsknn tc: mode=%d n=%d m=%d d=%d k=%d S=%d N=%d: logged/query=%.1f "
+                 "gsknn tc: mode=%d n=%d m=%d d=%d k=%d S=%d N=%d NST=%d: logged/query=%.1f "
                  "inserts/query=%.1f loop-iters/warp=%.1f slow-chunks/warp=%.1f "
-                 "chunks/warp=%.1f rerank-scanned/query=%.1f exact/query=%.1f fallback=%d\n",
-                 mode, nq, nc, d, k, P.S, P.N, (double)h[0] / nq, (double)h[1] / nq,
-                 (double)h[2] / (P.qtiles * P.S * 8.0), (double)h[3] / (P.qtiles * P.S * 8.0),
-                 (double)h[4] / (P.qtiles * P.S * 8.0), (double)h[5] / nq, (double)h[6] / nq,
-                 nfb);
+                 "chunks/warp=%.1f rerank-scanned/query=%.1f exact/query=%.1f fallback=%d | "
+                 "cycles/CTA: mma-loop=%.0f mma-wait-tma=%.0f mma-wait-epilogue=%.0f | "
+                 "cycles/warp: epi-loop=%.0f epi-wait-mma=%.0f\n",
+                 mode, nq, nc, d, k, P.S, P.N, P.NST, (double)h[0] / nq, (double)h[1] / nq,
+                 (double)h[2] / warps, (double)h[3] / warps, (double)h[4] / warps,
+                 (double)h[5] / nq, (double)h[6] / nq, nfb, (double)h[10] / ctas,
+                 (double)h[7] / ctas, (double)h[8] / ctas, (double)h[11] / warps,
+                 (double)h[9] / warps);
   }
   if (margin)
     CU(cudaMemcpyAsync(margin, static_cast<char *>(ws) + P.o_margin, (size_t)nq * 4,
@@ -450,29 +517,6 @@ int knn_host(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, const int 
     qlo = clo = std::min(qlo, clo);
     qhi = chi = std::max(qhi, chi);
   }
-  auto copy_table = [&](int slot_t, int slot_n, const T *X, const T *X2, int lo, int hi,
-                        const T **dX, const T **dX2) -> int {
-    const size_t rows = (size_t)(hi - lo + 1);
-    void *pt = nullptr, *pn = nullptr;
-    CU(scratch(slot_t, rows * d * sizeof(T), st, &pt));
-    CU(scratch(slot_n, rows * sizeof(T), st, &pn));
-    CU(cudaMemcpyAsync(pt, X + (size_t)lo * d, rows * d * sizeof(T), cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(pn, X2 + lo, rows * sizeof(T), cudaMemcpyHostToDevice, st));
-    // offset so that global row ids index the copied range directly
-    *dX = static_cast<const T *>(pt) - (size_t)lo * d;
-    *dX2 = static_cast<const T *>(pn) - lo;
-    return 0;
-  };
-  const T *dXq, *dXq2, *dXc, *dXc2;
-  int rc = copy_table(SLOT_HQTAB, SLOT_HQNRM, Xq, Xq2, qlo, qhi, &dXq, &dXq2);
-  if (rc) return rc;
-  if (same) {
-    dXc = dXq;
-    dXc2 = dXq2;
-  } else {
-    rc = copy_table(SLOT_HCTAB, SLOT_HCNRM, Xc, Xc2, clo, chi, &dXc, &dXc2);
-    if (rc) return rc;
-  }
   void *pqi, *pci, *pD, *pI;
   CU(scratch(SLOT_HQIDX, (size_t)nq * 4, st, &pqi));
   CU(scratch(SLOT_HCIDX, (size_t)nc * 4, st, &pci));
@@ -480,6 +524,59 @@ int knn_host(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, const int 
   CU(scratch(SLOT_HI, (size_t)nq * ldD * 4, st, &pI));
   CU(cudaMemcpyAsync(pqi, qidx, (size_t)nq * 4, cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync(pci, cidx, (size_t)nc * 4, cudaMemcpyHostToDevice, st));
+  // Device copy of each table over the row range the index lists reach, so that global row ids
+  // index it directly. When the lists reference well under that range (random subsets of a
+  // large table), only the referenced rows travel: gathered on the host into pinned staging,
+  // one copy, then scattered into place on the device. Otherwise the range is copied as is.
+  const size_t qrows = (size_t)(qhi - qlo + 1), crows = (size_t)(chi - clo + 1);
+  const size_t range_rows = same ? qrows : qrows + crows;
+  const bool sparse = (size_t)(nq + nc) * 10 < range_rows * 6;
+  void *pqt = nullptr, *pqn = nullptr, *pct = nullptr, *pcn = nullptr;
+  CU(scratch(SLOT_HQTAB, qrows * d * sizeof(T), st, &pqt));
+  CU(scratch(SLOT_HQNRM, qrows * sizeof(T), st, &pqn));
+  if (!same) {
+    CU(scratch(SLOT_HCTAB, crows * d * sizeof(T), st, &pct));
+    CU(scratch(SLOT_HCNRM, crows * sizeof(T), st, &pcn));
+  } else {
+    pct = pqt;
+    pcn = pqn;
+  }
+  if (sparse) {
+    const size_t n = (size_t)nq + nc;
+    const size_t bytes = n * d * sizeof(T) + n * sizeof(T);
+    void *stage = nullptr, *dg = nullptr;
+    CU(cudaStreamSynchronize(st));  // the staging buffer of the previous call is free
+    CU(pinned_stage(bytes, &stage));
+    CU(scratch(SLOT_HGATHER, bytes, st, &dg));
+    T *hrows = static_cast<T *>(stage);
+    T *hn = hrows + n * d;
+    gather_rows<T>(Xq, Xq2, d, qidx, nq, hrows, hn);
+    gather_rows<T>(Xc, Xc2, d, cidx, nc, hrows + (size_t)nq * d, hn + nq);
+    CU(cudaMemcpyAsync(dg, stage, bytes, cudaMemcpyHostToDevice, st));
+    const T *grows = static_cast<const T *>(dg);
+    const T *gn = grows + n * d;
+    scatter_rows<T><<<(nq + 7) / 8, 256, 0, st>>>(grows, gn, static_cast<const int *>(pqi), nq,
+                                                  d, qlo, static_cast<T *>(pqt),
+                                                  static_cast<T *>(pqn));
+    scatter_rows<T><<<(nc + 7) / 8, 256, 0, st>>>(grows + (size_t)nq * d, gn + nq,
+                                                  static_cast<const int *>(pci), nc, d, clo,
+                                                  static_cast<T *>(pct), static_cast<T *>(pcn));
+    CU(cudaGetLastError());
+  } else {
+    CU(cudaMemcpyAsync(pqt, Xq + (size_t)qlo * d, qrows * d * sizeof(T), cudaMemcpyHostToDevice,
+                       st));
+    CU(cudaMemcpyAsync(pqn, Xq2 + qlo, qrows * sizeof(T), cudaMemcpyHostToDevice, st));
+    if (!same) {
+      CU(cudaMemcpyAsync(pct, Xc + (size_t)clo * d, crows * d * sizeof(T),
+                         cudaMemcpyHostToDevice, st));
+      CU(cudaMemcpyAsync(pcn, Xc2 + clo, crows * sizeof(T), cudaMemcpyHostToDevice, st));
+    }
+  }
+  const T *dXq = static_cast<const T *>(pqt) - (size_t)qlo * d;
+  const T *dXq2 = static_cast<const T *>(pqn) - qlo;
+  const T *dXc = static_cast<const T *>(pct) - (size_t)clo * d;
+  const T *dXc2 = static_cast<const T *>(pcn) - clo;
+  int rc = GSKNN_OK;
   CU(cudaMemcpyAsync(pD, D, (size_t)nq * ldD * sizeof(T), cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync(pI, I, (size_t)nq * ldD * 4, cudaMemcpyHostToDevice, st));
   if (path == 0)

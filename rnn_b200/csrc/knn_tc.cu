@@ -45,6 +45,10 @@ constexpr int A_CHUNK = TC_M * CHUNK_BYTES;  // 16 KB
 constexpr int NEPI = 8;
 constexpr int NTHREADS = 32 * (2 + NEPI);
 constexpr uint32_t LOG_OVF = 1u << 30;
+// The epilogue frees a TMEM accumulator as soon as its reads have landed, while it still uses
+// the tile's candidate norms; the norms therefore get one slot more than the two accumulators
+// (the slot the MMA warp refills belongs to a tile every epilogue warp has finished).
+constexpr int CN_SLOTS = 3;
 
 // ------------------------------------------------------------------------------------------
 // shift vector
@@ -207,11 +211,11 @@ __host__ __device__ inline SmemLayout tc_smem_layout(int nkc, int a_terms, int b
   L.heap_off = off;
   off += (uint32_t)k * TC_M * 4;
   off = (off + 15) & ~15u;
-  L.cn_off = off;  // candidate norms of the two tiles in TMEM, copied by the MMA warp
-  off += 2u * N * 4;
+  L.cn_off = off;  // candidate norms of the tiles in flight, copied by the MMA warp
+  off += (uint32_t)CN_SLOTS * N * 4;
   off = (off + 7) & ~7u;
   L.bar_off = off;
-  off += (uint32_t)(2 * NST + 7) * 8;
+  off += (uint32_t)(2 * NST + 5 + CN_SLOTS) * 8;  // full, empty, tfull[2], tempty[2], afull, cnfull
   L.tmem_off = off;
   off += 16;
   L.total = off + 1024;  // alignment slack
@@ -359,8 +363,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       mbar_init(&tempty[b], NEPI);
     }
     mbar_init(afull, 1);
-    mbar_init(&cnfull[0], 1);
-    mbar_init(&cnfull[1], 1);
+    for (int c = 0; c < CN_SLOTS; c++) mbar_init(&cnfull[c], 1);
     mbar_fence_init();
   }
   if (warp == 1) {
@@ -403,6 +406,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
     if (lane == 0 && ntile > 0) {
+      const long long t_start = p.counters ? clock64() : 0;
+      long long w_tempty = 0, w_full = 0;
       if (!mbar_wait(afull, 0)) failed = true;
       tc_fence_after();
       const uint32_t a_base = su32(sA), b_base = su32(sB);
@@ -410,16 +415,22 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       for (int lt = 0; lt < ntile && !failed; lt++) {
         const int b = lt & 1;
         const uint32_t use = (uint32_t)(lt >> 1);
+        long long t0 = p.counters ? clock64() : 0;
         if (!mbar_wait(&tempty[b], (use & 1u) ^ 1u)) { failed = true; break; }
-        // buffer b is free, so is its norm slot: fetch this tile's candidate norms
-        mbar_expect_tx(&cnfull[b], (uint32_t)(N * 4));
-        bulk_g2s(cn_s + b * N, p.cn + (size_t)(t_begin + lt) * N, (uint32_t)(N * 4), &cnfull[b]);
+        if (p.counters) w_tempty += clock64() - t0;
+        // every epilogue warp has released tile lt - 2, so all of them are done with tile lt - 3
+        // and its norm slot: fetch this tile's candidate norms there
+        const int c = lt % CN_SLOTS;
+        mbar_expect_tx(&cnfull[c], (uint32_t)(N * 4));
+        bulk_g2s(cn_s + c * N, p.cn + (size_t)(t_begin + lt) * N, (uint32_t)(N * 4), &cnfull[c]);
         tc_fence_after();
         const uint32_t tmem_d = tmem_base + (uint32_t)(b * N);
         for (int kc = 0; kc < p.nkc; kc++, it++) {
           const int s = it % p.NST;
           const uint32_t round = (uint32_t)(it / p.NST);
+          t0 = p.counters ? clock64() : 0;
           if (!mbar_wait(&full[s], round & 1u)) { failed = true; break; }
+          if (p.counters) w_full += clock64() - t0;
           tc_fence_after();
           const uint32_t a_chunk = a_base + (uint32_t)kc * A_CHUNK;
           const uint32_t b_chunk = b_base + (uint32_t)s * b_stage_bytes;
@@ -444,6 +455,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           mma_commit(&empty[s]);
         }
         if (!failed) mma_commit(&tfull[b]);
+      }
+      if (p.counters) {
+        atomicAdd(&p.counters[7], (unsigned long long)w_full);
+        atomicAdd(&p.counters[8], (unsigned long long)w_tempty);
+        atomicAdd(&p.counters[10], (unsigned long long)(clock64() - t_start));
       }
     }
   } else {
@@ -497,23 +513,23 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     // One 32-column chunk: approximate distances, a cheap min-filter, and for the rare chunks
     // with survivors a warp-convergent pass in which every lane with pending candidates handles
     // one of them per iteration (selected from its registers by index).
-    auto chunk = [&](const uint32_t (&r)[32], const float *cnt, size_t cbase, int c0) {
-      float v[32];
+    // d' - qn' (the v space) is written over the accumulator values in place (r is consumed)
+    auto chunk = [&](uint32_t (&r)[32], const float *cnt, size_t cbase, int c0) {
       float mn = Num<float>::inf();
       const float4 *cn4 = reinterpret_cast<const float4 *>(cnt + c0);
 #pragma unroll
       for (int j = 0; j < 8; j++) {
         const float4 c4 = cn4[j];
-        v[4 * j + 0] = fmaf(__uint_as_float(r[4 * j + 0]), -2.0f, c4.x);
-        v[4 * j + 1] = fmaf(__uint_as_float(r[4 * j + 1]), -2.0f, c4.y);
-        v[4 * j + 2] = fmaf(__uint_as_float(r[4 * j + 2]), -2.0f, c4.z);
-        v[4 * j + 3] = fmaf(__uint_as_float(r[4 * j + 3]), -2.0f, c4.w);
+        r[4 * j + 0] = __float_as_uint(fmaf(__uint_as_float(r[4 * j + 0]), -2.0f, c4.x));
+        r[4 * j + 1] = __float_as_uint(fmaf(__uint_as_float(r[4 * j + 1]), -2.0f, c4.y));
+        r[4 * j + 2] = __float_as_uint(fmaf(__uint_as_float(r[4 * j + 2]), -2.0f, c4.z));
+        r[4 * j + 3] = __float_as_uint(fmaf(__uint_as_float(r[4 * j + 3]), -2.0f, c4.w));
       }
       {
         // tree minimum: depth 5 instead of a 32-long dependency chain
         float m16[16];
 #pragma unroll
-        for (int j = 0; j < 16; j++) m16[j] = fminf(v[2 * j], v[2 * j + 1]);
+        for (int j = 0; j < 16; j++) m16[j] = fminf(__uint_as_float(r[2 * j]), __uint_as_float(r[2 * j + 1]));
 #pragma unroll
         for (int w = 8; w >= 1; w >>= 1)
 #pragma unroll
@@ -523,7 +539,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       if (p.dbg && valid) {
         for (int i = 0; i < 32; i++) {
           const long long col = (long long)cbase + c0 + i;
-          if (col < p.dbg_ncols) p.dbg[(size_t)gq * p.dbg_ld + col] = v[i] + s.qn;
+          if (col < p.dbg_ncols) p.dbg[(size_t)gq * p.dbg_ld + col] = __uint_as_float(r[i]) + s.qn;
         }
       }
       if (!__any_sync(FULL_MASK, mn <= s.Tv)) return;
@@ -540,8 +556,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         uint32_t m16[16];
 #pragma unroll
         for (int j = 0; j < 16; j++)
-          m16[j] = (v[2 * j] <= s.Tv ? 1u << (2 * j) : 0u) |
-                   (v[2 * j + 1] <= s.Tv ? 1u << (2 * j + 1) : 0u);
+          m16[j] = (__uint_as_float(r[2 * j]) <= s.Tv ? 1u << (2 * j) : 0u) |
+                   (__uint_as_float(r[2 * j + 1]) <= s.Tv ? 1u << (2 * j + 1) : 0u);
 #pragma unroll
         for (int w = 8; w >= 1; w >>= 1)
 #pragma unroll
@@ -557,7 +573,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           // v[i] for a runtime i: a 5-level select tree on the bits of i
           float t16[16];
 #pragma unroll
-          for (int j = 0; j < 16; j++) t16[j] = (i & 16) ? v[j + 16] : v[j];
+          for (int j = 0; j < 16; j++)
+            t16[j] = __uint_as_float((i & 16) ? r[j + 16] : r[j]);
 #pragma unroll
           for (int w = 8, bit = 8; w >= 1; w >>= 1, bit >>= 1)
 #pragma unroll
@@ -573,9 +590,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     // what the query's other splits have found (all bits set = nothing yet); the load for the
     // next tile is issued a tile ahead so its latency hides behind the tile's work
     unsigned sh_next = valid ? __ldcg(ksh) : 0xFFFFFFFFu;
+    const long long t_start = p.counters ? clock64() : 0;
+    long long w_tfull = 0;
     for (int lt = 0; lt < ntile && !failed; lt++) {
-      const int b = lt & 1;
-      const uint32_t use = (uint32_t)(lt >> 1);
+      const int b = lt & 1, c = lt % CN_SLOTS;
+      const uint32_t use = (uint32_t)(lt >> 1), cuse = (uint32_t)(lt / CN_SLOTS);
       if (valid) {
         const float sh = __uint_as_float(sh_next);
         if (sh < s.shared) {
@@ -584,12 +603,18 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         }
         sh_next = __ldcg(ksh);
       }
+      const long long t0 = p.counters ? clock64() : 0;
       if (!mbar_wait(&tfull[b], use & 1u)) { failed = true; break; }
-      if (!mbar_wait(&cnfull[b], use & 1u)) { failed = true; break; }
+      if (!mbar_wait(&cnfull[c], cuse & 1u)) { failed = true; break; }
+      if (p.counters) w_tfull += clock64() - t0;
       tc_fence_after();
       const uint32_t taddr = tmem_base + ((uint32_t)(lq * 32) << 16) + (uint32_t)(b * N);
+      const float *cnt = cn_s + c * N;
       const int tile = t_begin + lt;
       const size_t cbase = (size_t)tile * N;
+      // this warp's N/2 columns, 64 at a time (two 32-column chunks per TMEM wait); the
+      // accumulator is freed for the MMA warp once the tile's last loads have landed (the norms
+      // stay in their own slot)
       const int cb = half * (N / 2), ce = cb + N / 2;
       for (int c0 = cb; c0 < ce; c0 += 64) {
         uint32_t ra[32], rb[32];
@@ -597,12 +622,16 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         tmem_ld32(taddr + (uint32_t)c0, ra);
         tmem_ld32(taddr + (uint32_t)c0 + 32u, rb);
         tmem_wait_ld();
-        chunk(ra, cn_s + b * N, cbase, c0);
-        chunk(rb, cn_s + b * N, cbase, c0 + 32);
+        reg_fence32(ra);
+        reg_fence32(rb);
+        if (c0 + 64 >= ce) {
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&tempty[b]);
+        }
+        chunk(ra, cnt, cbase, c0);
+        chunk(rb, cnt, cbase, c0 + 32);
       }
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&tempty[b]);
     }
     if (owner) epi_flush(s, heap, row, p.k, pend, np, ksh);
     if (valid) {
@@ -616,6 +645,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         atomicAdd(&p.counters[2], (unsigned long long)s.n_it);
         atomicAdd(&p.counters[3], (unsigned long long)s.n_sc);
         atomicAdd(&p.counters[4], (unsigned long long)ntile * (N / 64));
+        atomicAdd(&p.counters[9], (unsigned long long)w_tfull);
+        atomicAdd(&p.counters[11], (unsigned long long)(clock64() - t_start));
       }
     }
   }
