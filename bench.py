@@ -394,10 +394,8 @@ def run_ours(args, rank, world, local_rank):
     peaks = load_peaks()
     name2mode = {v: k for k, v in MODE_NAMES.items()}
 
-    def barrier():
-        if world > 1:
-            import torch.distributed as dist
-            dist.barrier()
+    from rnn_b200 import replicas as RP
+    barrier = RP.barrier
 
     out = {}
     if args.batch_only:
@@ -407,22 +405,15 @@ def run_ours(args, rank, world, local_rank):
     if not args.precision_only:
         p = W.config2(seed=2)
         nq = args.queries
-        if world > 1:
-            beta_h = W.permutation(1000 + rank, N_POINTS)[:nq].astype(np.int32)
-        else:
-            beta_h = np.ascontiguousarray(p.beta[:nq])
+        beta_h = RP.replica_queries(rank, world, N_POINTS, nq, default=p.beta)
         prob = DeviceProblem(p, beta_h, dev)
         clocks = ClockSampler(local_rank) if not args.profile_only else None
         mode = name2mode[args.mode]
         ms, trace = timed(L, G, prob, mode, args.steps, args.warmup, barrier, clocks)
         clk = clocks.stop() if clocks else None
-        if world > 1:
-            import torch.distributed as dist
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = RP.max_over_ranks(ms, device=dev)
         used = effective_mode_name(trace, p.d)
-        value = prob.evals * world / (ms * 1e-3)
+        value = RP.job_throughput(prob.evals, world, ms)
         out = {
             "metric": "distance-evals/s", "value": value, "unit": "distance-evals/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
