@@ -93,6 +93,8 @@ def parse():
     ap.add_argument("--serve-refs", type=int, default=1 << 22,
                     help="resident reference points of the serving workload")
     ap.add_argument("--serve-requests", type=int, default=400)
+    ap.add_argument("--serve-mode", default="auto", choices=list(MODE_NAMES.values()),
+                    help="arithmetic of the serving engine (a tensor-core mode or auto)")
     ap.add_argument("--serve-rate", type=float, default=150.0,
                     help="mean request arrival rate (requests/s, Poisson)")
     ap.add_argument("--cpu-worker", default=None, help=argparse.SUPPRESS)
@@ -467,7 +469,7 @@ def effective_mode_name(trace, d):
     from rnn_b200 import gsknn as G
     m = G.get_mode()
     if m == 0:
-        return "bf16x3" if d < 128 else "tf32"
+        return "bf16x3" if d <= 256 else "tf32"  # AUTO: split BF16 where its tiles fit
     return MODE_NAMES[m]
 
 
@@ -582,8 +584,9 @@ def serving_form(L, G, W, dev, args):
     ms = np.floor(np.exp(rng.uniform(0.0, np.log(4096.0), size=n))).astype(int).clip(1, 4096)
     ks = rng.choice([8, 16, 64], size=n)
     qs = [W.uniform_table(5000 + i, int(ms[i]), d).astype(np.float32) for i in range(n)]
-    srv = SV.Server(Rd, R2d, mode=0, max_batch_queries=8192, max_k=64, heap_budget=2 << 30,
-                    slots=3)
+    serve_mode = {v: k for k, v in MODE_NAMES.items()}[args.serve_mode]
+    srv = SV.Server(Rd, R2d, mode=serve_mode, max_batch_queries=8192, max_k=64,
+                    heap_budget=2 << 30, slots=3)
     for m_w in (1, 128, 4096):  # warm-up: module loads, first launches of every kernel
         rid = srv.submit(W.uniform_table(99, m_w, d).astype(np.float32), 64)
         srv.wait(rid)
@@ -638,7 +641,8 @@ def serving_form(L, G, W, dev, args):
         "workload": (f"serving: resident refs={nref} d={d} U[0,1); {n} requests, Poisson "
                      f"{args.serve_rate:g}/s, m log-uniform [1,4096] (mean {ms.mean():.0f}), "
                      f"k in {{8,16,64}}"),
-        "dtype": "f32 inputs; tf32 tensor distances + fp64 re-rank (exact top-k)",
+        "dtype": f"f32 inputs; {args.serve_mode} tensor distances + fp64 re-rank (exact top-k)"
+                 + (" [auto = split bf16 here]" if args.serve_mode == "auto" else ""),
         "latency_ms": summary(lat, queue, ms),
         "value": evals / wall, "unit": "distance-evals/s",
         "wall_s": wall, "mean_batch_rows": float(np.mean(rows)),

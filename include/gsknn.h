@@ -146,7 +146,9 @@ const char *gsknn_last_error_string(void);
  *   GSKNN_MODE_FP32 -- CUDA-core FP32 distances;
  *   GSKNN_MODE_TF32, GSKNN_MODE_BF16 -- tensor-core distances with an FP64 re-rank of every
  *     candidate within the rounding bound of the k-th distance (exact index sets);
- *   GSKNN_MODE_AUTO -- the faster exact choice for the problem shape (default). */
+ *   GSKNN_MODE_AUTO -- split BF16 where its tiles fit in shared memory (the narrowest re-rank
+ *     band; measured fastest of the exact forms at d = 64 and 256), else TF32, else FP32
+ *     (default). */
 #define GSKNN_MODE_AUTO 0
 #define GSKNN_MODE_FP32 1
 #define GSKNN_MODE_TF32 2
@@ -265,7 +267,7 @@ void gsknn_batch_forget_tuning(void);
  *
  * gsknn_serve_create prepares the nref x d float reference set R (device pointer, with norms
  * R2) once: packed for the tensor cores (mode AUTO / TF32 / BF16 / BF16X3; AUTO = split BF16
- * below d = 128, TF32 from there) and resident until destroy. Each request is m query rows
+ * where its tiles fit, else TF32) and resident until destroy. Each request is m query rows
  * (host memory, copied at submit) and a k <= max_k; its result is the exact FP64 top-k of every
  * query against R (ties to the lower id), as a heap of m rows x k (descending rows) that stays
  * on the device until the request is released.

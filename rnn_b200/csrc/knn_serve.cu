@@ -321,7 +321,10 @@ gsknn_serve_t *gsknn_serve_create(const float *R, const float *R2, int nref, int
     serr(GSKNN_ERR_ARG, "gsknn_serve_create: invalid argument");
     return nullptr;
   }
-  if (mode == GSKNN_MODE_AUTO) mode = d < 128 ? GSKNN_MODE_BF16X3 : GSKNN_MODE_TF32;
+  if (mode == GSKNN_MODE_AUTO)
+    mode = tc_plan(max_batch_queries, nref, d, max_k, GSKNN_TC_BF16X3, 148, false, 148).ok
+               ? GSKNN_MODE_BF16X3
+               : GSKNN_MODE_TF32;
   if (mode < GSKNN_MODE_TF32 || mode > GSKNN_MODE_BF16X3) {
     serr(GSKNN_ERR_ARG, "gsknn_serve_create: mode must be AUTO, TF32, BF16 or BF16X3");
     return nullptr;

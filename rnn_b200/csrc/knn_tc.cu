@@ -370,6 +370,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     tmem_alloc(tmem_holder, (uint32_t)(2 * N));
     tmem_relinquish();
   }
+  // the per-row heaps start at +inf before any epilogue warp reads a root (the log-only warp of
+  // a row reads its owner's root as a threshold)
+  for (int i = threadIdx.x; i < p.k * TC_M; i += NTHREADS) heap[i] = Num<float>::inf();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -470,8 +473,6 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     const int row = lq * 32 + lane;
     const int gq = qt * TC_M + row;
     const bool valid = gq < p.Q;
-    if (owner)
-      for (int i = 0; i < p.k; i++) heap[i * TC_M + row] = Num<float>::inf();
     EpiState s;
     s.cnt = 0;
     s.ovf = 0;
@@ -513,8 +514,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     // One 32-column chunk: approximate distances, a cheap min-filter, and for the rare chunks
     // with survivors a warp-convergent pass in which every lane with pending candidates handles
     // one of them per iteration (selected from its registers by index).
-    // d' - qn' (the v space) is written over the accumulator values in place (r is consumed)
-    auto chunk = [&](uint32_t (&r)[32], const float *cnt, size_t cbase, int c0) {
+    // Fast part of a 32-column chunk: d' - qn' (the v space) over the accumulator values in
+    // place, and their minimum (a tree of depth 5). Two chunks' fast parts run back to back in
+    // one basic block so their independent arithmetic overlaps.
+    auto fast = [&](uint32_t (&r)[32], const float *cnt, int c0) -> float {
       float mn = Num<float>::inf();
       const float4 *cn4 = reinterpret_cast<const float4 *>(cnt + c0);
 #pragma unroll
@@ -536,13 +539,18 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           for (int j = 0; j < w; j++) m16[j] = fminf(m16[2 * j], m16[2 * j + 1]);
         mn = m16[0];
       }
-      if (p.dbg && valid) {
-        for (int i = 0; i < 32; i++) {
-          const long long col = (long long)cbase + c0 + i;
-          if (col < p.dbg_ncols) p.dbg[(size_t)gq * p.dbg_ld + col] = __uint_as_float(r[i]) + s.qn;
-        }
+      return mn;
+    };
+    auto dbg_write = [&](const uint32_t (&r)[32], size_t cbase, int c0) {
+      for (int i = 0; i < 32; i++) {
+        const long long col = (long long)cbase + c0 + i;
+        if (col < p.dbg_ncols) p.dbg[(size_t)gq * p.dbg_ld + col] = __uint_as_float(r[i]) + s.qn;
       }
-      if (!__any_sync(FULL_MASK, mn <= s.Tv)) return;
+    };
+    // Slow part, for a chunk in which some lane has a candidate under its threshold: a
+    // warp-convergent pass in which every lane with pending candidates handles one of them per
+    // iteration (selected from its registers by index).
+    auto slow = [&](const uint32_t (&r)[32], size_t cbase, int c0, float mn) {
       // a chunk appends at most 32 entries per lane: make room first, all lanes together
       if (__any_sync(FULL_MASK, s.cnt > p.logcap - 32)) {
         if (s.cnt > p.logcap - 32 && !s.ovf) {
@@ -597,10 +605,21 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       const uint32_t use = (uint32_t)(lt >> 1), cuse = (uint32_t)(lt / CN_SLOTS);
       if (valid) {
         const float sh = __uint_as_float(sh_next);
+        bool tighter = false;
         if (sh < s.shared) {
           s.shared = sh;
-          refresh_threshold(s);
+          tighter = true;
         }
+        if (!owner) {
+          // the row's owner warp (same TMEM lane quarter, other half of the columns) keeps the
+          // heap: its root bounds this warp's threshold too (one 4-byte word, written whole)
+          const float ro = *reinterpret_cast<volatile const float *>(&heap[row]);
+          if (ro < s.root) {
+            s.root = ro;
+            tighter = true;
+          }
+        }
+        if (tighter) refresh_threshold(s);
         sh_next = __ldcg(ksh);
       }
       const long long t0 = p.counters ? clock64() : 0;
@@ -629,8 +648,14 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           __syncwarp();
           if (lane == 0) mbar_arrive(&tempty[b]);
         }
-        chunk(ra, cnt, cbase, c0);
-        chunk(rb, cnt, cbase, c0 + 32);
+        const float ma = fast(ra, cnt, c0);
+        const float mb = fast(rb, cnt, c0 + 32);
+        if (p.dbg && valid) {
+          dbg_write(ra, cbase, c0);
+          dbg_write(rb, cbase, c0 + 32);
+        }
+        if (__any_sync(FULL_MASK, ma <= s.Tv)) slow(ra, cbase, c0, ma);
+        if (__any_sync(FULL_MASK, mb <= s.Tv)) slow(rb, cbase, c0 + 32, mb);
       }
     }
     if (owner) epi_flush(s, heap, row, p.k, pend, np, ksh);
