@@ -518,28 +518,30 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     // place, and their minimum (a tree of depth 5). Two chunks' fast parts run back to back in
     // one basic block so their independent arithmetic overlaps.
     auto fast = [&](uint32_t (&r)[32], const float *cnt, int c0) -> float {
-      float mn = Num<float>::inf();
       const float4 *cn4 = reinterpret_cast<const float4 *>(cnt + c0);
 #pragma unroll
       for (int j = 0; j < 8; j++) {
         const float4 c4 = cn4[j];
-        r[4 * j + 0] = __float_as_uint(fmaf(__uint_as_float(r[4 * j + 0]), -2.0f, c4.x));
-        r[4 * j + 1] = __float_as_uint(fmaf(__uint_as_float(r[4 * j + 1]), -2.0f, c4.y));
-        r[4 * j + 2] = __float_as_uint(fmaf(__uint_as_float(r[4 * j + 2]), -2.0f, c4.z));
-        r[4 * j + 3] = __float_as_uint(fmaf(__uint_as_float(r[4 * j + 3]), -2.0f, c4.w));
+        float v0, v1, v2, v3;
+        fma2(v0, v1, __uint_as_float(r[4 * j + 0]), __uint_as_float(r[4 * j + 1]), -2.0f, c4.x,
+             c4.y);
+        fma2(v2, v3, __uint_as_float(r[4 * j + 2]), __uint_as_float(r[4 * j + 3]), -2.0f, c4.z,
+             c4.w);
+        r[4 * j + 0] = __float_as_uint(v0);
+        r[4 * j + 1] = __float_as_uint(v1);
+        r[4 * j + 2] = __float_as_uint(v2);
+        r[4 * j + 3] = __float_as_uint(v3);
       }
-      {
-        // tree minimum: depth 5 instead of a 32-long dependency chain
-        float m16[16];
+      // minimum: three-input tree of depth 4 (32 -> 11 -> 4 -> 1)
+      float m11[11];
 #pragma unroll
-        for (int j = 0; j < 16; j++) m16[j] = fminf(__uint_as_float(r[2 * j]), __uint_as_float(r[2 * j + 1]));
-#pragma unroll
-        for (int w = 8; w >= 1; w >>= 1)
-#pragma unroll
-          for (int j = 0; j < w; j++) m16[j] = fminf(m16[2 * j], m16[2 * j + 1]);
-        mn = m16[0];
-      }
-      return mn;
+      for (int j = 0; j < 10; j++)
+        m11[j] = fmin3(__uint_as_float(r[3 * j]), __uint_as_float(r[3 * j + 1]),
+                       __uint_as_float(r[3 * j + 2]));
+      m11[10] = fminf(__uint_as_float(r[30]), __uint_as_float(r[31]));
+      const float n0 = fmin3(m11[0], m11[1], m11[2]), n1 = fmin3(m11[3], m11[4], m11[5]);
+      const float n2 = fmin3(m11[6], m11[7], m11[8]), n3 = fminf(m11[9], m11[10]);
+      return fminf(fmin3(n0, n1, n2), n3);
     };
     auto dbg_write = [&](const uint32_t (&r)[32], size_t cbase, int c0) {
       for (int i = 0; i < 32; i++) {

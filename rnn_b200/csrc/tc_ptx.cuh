@@ -123,6 +123,25 @@ __device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t adesc, uint64_
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
       : "memory");
 }
+// Packed FP32 pair arithmetic of sm_100: (d0, d1) = (a0 * m + c0, a1 * m + c1), each rounded to
+// nearest like fmaf; and the minimum of three floats (NaN operands ignored, as fminf).
+__device__ __forceinline__ void fma2(float &d0, float &d1, float a0, float a1, float m, float c0,
+                                     float c1) {
+  asm("{\n\t.reg .b64 ra, rm, rc, rd;\n\t"
+      "mov.b64 ra, {%2, %3};\n\t"
+      "mov.b64 rm, {%4, %4};\n\t"
+      "mov.b64 rc, {%5, %6};\n\t"
+      "fma.rn.f32x2 rd, ra, rm, rc;\n\t"
+      "mov.b64 {%0, %1}, rd;\n\t}\n"
+      : "=f"(d0), "=f"(d1)
+      : "f"(a0), "f"(a1), "f"(m), "f"(c0), "f"(c1));
+}
+__device__ __forceinline__ float fmin3(float a, float b, float c) {
+  float r;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+
 // Arrive on `bar` once all previously issued tcgen05.mma of this thread have completed.
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
   asm volatile(
