@@ -312,6 +312,42 @@ int gsknn_rkdt_leaves(const float *X, int N, int d, int ntrees, int leaf_min, in
                       unsigned long long seed, int threads, int *leaf_ptr, int *leaf_pts,
                       int *leaf_tree, int max_leaves, int *nleaves);
 
+/* ---- Sorted-output adapters: replace frame/old/dgsrnn_directKQuery.cpp:14-135
+ *      (dgsrnn_directKQuery) and 141-222 (dgsrnn_directKQuery_var2) ----
+ * The reference returns std::pair<double, long> lists; a C ABI cannot, so each list is two
+ * row-major m x k arrays: dist (squared distances) and id (64-bit point ids, -1 = none).
+ *
+ * gsknn_direct_kquery_d/_s(ref, query, n, m, k, dim, dist, id): all m queries (rows of `query`,
+ * m x dim) against all n references (rows of `ref`, n x dim), norms computed here; row i of the
+ * result is query i's k nearest references in ascending (distance, id) order, as the
+ * reference's heap pops produce (dgsrnn_directKQuery.cpp:112-124; exact ties ordered by id).
+ * With n < k the last entries are (largest finite value, -1), the reference's initial heap
+ * (dgsrnn_directKQuery.cpp:50-53). Arithmetic as dgsknn_var1 / sgsknn_var1.
+ *
+ * gsknn_direct_kquery_maps_d/_s(m, n, dim, k, query, XA2, amap, ref, XB2, bmap, dist, id): the
+ * _var2 form: queries amap[0..m) of `query` with norms XA2, references bmap[0..n) of `ref` with
+ * norms XB2; rows left in heap order (max-heaps, descending here), as the reference copies them.
+ *
+ * Both take host pointers, block until done and return 0, GSKNN_EARLY_RETURN (a size is 0) or
+ * an error code (also in gsknn_last_error()). */
+int gsknn_direct_kquery_d(const double *ref, const double *query, long n, long m, long k,
+                          long dim, double *dist, long *id);
+int gsknn_direct_kquery_s(const float *ref, const float *query, long n, long m, long k, long dim,
+                          float *dist, long *id);
+int gsknn_direct_kquery_maps_d(int m, int n, int dim, int k, const double *query,
+                               const double *XA2, const int *amap, const double *ref,
+                               const double *XB2, const int *bmap, double *dist, long *id);
+int gsknn_direct_kquery_maps_s(int m, int n, int dim, int k, const float *query,
+                               const float *XA2, const int *amap, const float *ref,
+                               const float *XB2, const int *bmap, float *dist, long *id);
+
+/* Device heap rows to ascending lists in place: each of the n rows (stride ldk >= k) of D / I
+ * is sorted ascending by (distance, id), ids compared as unsigned so -1 entries come last among
+ * equal distances. k <= 512. Asynchronous on `stream`; returns 0 when enqueued. The device form
+ * of the heap pops of dgsrnn_directKQuery.cpp:112-124, for heaps that stay on the GPU. */
+int gsknn_heap_sort_s_device(float *D, int *I, int n, int k, int ldk, void *stream);
+int gsknn_heap_sort_d_device(double *D, int *I, int n, int k, int ldk, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

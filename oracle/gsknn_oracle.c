@@ -475,3 +475,26 @@ int oracle_is_maxheap4_d(int n, int k, int ld, const double *D, const int *I) {
   }
   return 1;
 }
+
+/* ------------------------------------------------------------------------------------------
+ * Heap rows to ascending lists by repeated pops (frame/old/dgsrnn_directKQuery.cpp:112-124):
+ * pass j sifts the root down over the first k - j entries, emits the root at position
+ * k - j - 1 and moves the last live entry to the root. The row (stride ld) is consumed; the
+ * list goes to Dout / Iout (n x k, ids widened to 64 bits as the reference's std::pair).
+ * ---------------------------------------------------------------------------------------- */
+#define DEFINE_POP_ROWS(NAME, T, SIFT)                                                      \
+  void NAME(int n, int k, int ld, T *D, int *I, T *Dout, long long *Iout) {                 \
+    for (int i = 0; i < n; i++) {                                                           \
+      T *d = D + (size_t)i * ld;                                                            \
+      int *id = I + (size_t)i * ld;                                                         \
+      for (int j = 0; j < k; j++) {                                                         \
+        SIFT(d, 0, k - j, id);                                                              \
+        Dout[(size_t)i * k + k - j - 1] = d[0];                                             \
+        Iout[(size_t)i * k + k - j - 1] = (long long)id[0];                                 \
+        d[0] = d[k - j - 1];                                                                \
+        id[0] = id[k - j - 1];                                                              \
+      }                                                                                     \
+    }                                                                                       \
+  }
+DEFINE_POP_ROWS(oracle_heap_pop_rows_d, double, sift_down_d)
+DEFINE_POP_ROWS(oracle_heap_pop_rows_s, float, sift_down_s)

@@ -94,6 +94,12 @@ int oracle_is_maxheap_d(int n, int k, int ld, const double *D);
 int oracle_is_maxheap_s(int n, int k, int ld, const float *D);
 int oracle_is_maxheap4_d(int n, int k, int ld, const double *D, const int *I);
 
+/* Pops of max-heap rows into ascending lists (frame/old/dgsrnn_directKQuery.cpp:112-124). */
+void oracle_heap_pop_rows_d(int n, int k, int ld, double *D, int *I, double *Dout,
+                            long long *Iout);
+void oracle_heap_pop_rows_s(int n, int k, int ld, float *D, int *I, float *Dout,
+                            long long *Iout);
+
 /* Number of OpenMP threads the oracle uses (0 = runtime default). */
 void oracle_set_threads(int nthreads);
 

@@ -123,6 +123,20 @@ class Oracle:
                                        _p(Iout))
         return Dout, Iout
 
+    def heap_pop_rows(self, D, I, k=None):
+        """Ascending (dist, id int64) lists popped from max-heap rows D / I (copies consumed),
+        as dgsrnn_directKQuery does (frame/old/dgsrnn_directKQuery.cpp:112-124)."""
+        n, ld = D.shape
+        k = ld if k is None else k
+        D = np.ascontiguousarray(D).copy()
+        I = np.ascontiguousarray(I, dtype=np.int32).copy()
+        Dout = np.empty((n, k), dtype=D.dtype)
+        Iout = np.empty((n, k), dtype=np.int64)
+        f = (self.lib.oracle_heap_pop_rows_d if D.dtype == np.float64
+             else self.lib.oracle_heap_pop_rows_s)
+        f(_i(n), _i(k), _i(ld), _p(D), _p(I), _p(Dout), _p(Iout))
+        return Dout, Iout
+
     def is_maxheap(self, D, k=None):
         n, ld = D.shape
         k = ld if k is None else k

@@ -234,3 +234,64 @@ def knn_device(XA, XA2, alpha, XB, XB2, beta, D, I, stream=None, check=True):
     if check:
         if L.gsknn_stream_status(ctypes.c_void_p(st.cuda_stream)) != 0:
             _raise_on_error(False)
+
+
+# ---- sorted-output adapters (frame/old/dgsrnn_directKQuery.cpp) ----------------------------
+def direct_kquery(ref, query, k):
+    """dgsrnn_directKQuery (frame/old/dgsrnn_directKQuery.cpp:14-135) on numpy tables: the k
+    nearest rows of `ref` (n x dim) for every row of `query` (m x dim), as (dist, id) arrays of
+    shape (m, k), each row ascending by (distance, id); ids int64, -1 past n. float64 tables run
+    the double library path, float32 the single one."""
+    L = lib()
+    ref = numpy.ascontiguousarray(ref)
+    query = numpy.ascontiguousarray(query)
+    assert ref.dtype == query.dtype and ref.dtype in (numpy.float32, numpy.float64)
+    assert ref.ndim == query.ndim == 2 and ref.shape[1] == query.shape[1]
+    n, dim = ref.shape
+    m = query.shape[0]
+    dist = numpy.empty((m, k), dtype=ref.dtype)
+    ids = numpy.empty((m, k), dtype=numpy.int64)
+    f = L.gsknn_direct_kquery_d if ref.dtype == numpy.float64 else L.gsknn_direct_kquery_s
+    cl = ctypes.c_long
+    rc = f(_p(ref), _p(query), cl(n), cl(m), cl(k), cl(dim), _p(dist), _p(ids))
+    if rc not in (0, EARLY_RETURN):
+        _raise_on_error(False)
+    return dist, ids
+
+
+def direct_kquery_maps(query, XA2, amap, ref, XB2, bmap, k):
+    """dgsrnn_directKQuery_var2 (frame/old/dgsrnn_directKQuery.cpp:141-222): queries amap of
+    `query` (norms XA2) against references bmap of `ref` (norms XB2); (dist, id) arrays of
+    shape (len(amap), k) left in heap order, as the reference copies them out."""
+    L = lib()
+    dt = query.dtype
+    for a in (query, XA2, ref, XB2):
+        assert a.dtype == dt and a.flags["C_CONTIGUOUS"]
+    for a in (amap, bmap):
+        assert a.dtype == numpy.int32 and a.flags["C_CONTIGUOUS"]
+    m, n = amap.size, bmap.size
+    dist = numpy.empty((m, k), dtype=dt)
+    ids = numpy.empty((m, k), dtype=numpy.int64)
+    f = L.gsknn_direct_kquery_maps_d if dt == numpy.float64 else L.gsknn_direct_kquery_maps_s
+    ci = ctypes.c_int
+    rc = f(ci(m), ci(n), ci(query.shape[1]), ci(k), _p(query), _p(XA2), _p(amap), _p(ref),
+           _p(XB2), _p(bmap), _p(dist), _p(ids))
+    if rc not in (0, EARLY_RETURN):
+        _raise_on_error(False)
+    return dist, ids
+
+
+def heap_sort_device(D, I, stream=None):
+    """Sort the heap rows of device tensors D / I (n, k) in place into ascending (distance, id)
+    lists (gsknn_heap_sort_*_device), asynchronously on `stream` (default: torch's current)."""
+    import torch
+    L = lib()
+    assert D.dim() == 2 and I.shape == D.shape and D.is_cuda and I.dtype == torch.int32
+    assert D.stride(1) == 1 and I.stride(1) == 1 and D.stride(0) == I.stride(0)
+    st = torch.cuda.current_stream(D.device) if stream is None else stream
+    f = L.gsknn_heap_sort_s_device if D.dtype == torch.float32 else L.gsknn_heap_sort_d_device
+    f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                  ctypes.c_void_p]
+    rc = f(D.data_ptr(), I.data_ptr(), D.shape[0], D.shape[1], D.stride(0), st.cuda_stream)
+    if rc not in (0, EARLY_RETURN):
+        _raise_on_error(False)

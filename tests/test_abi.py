@@ -123,3 +123,28 @@ def test_python_wrapper_checks_shapes():
         G.sgsknn(3, 4, X, X2, q, X, X2, q, D, I)  # D is 2 x 5, k = 4
     with pytest.raises(AssertionError):
         G.dgsknn(3, 5, X, X2, q, X, X2, q, D, I)  # float tables to the double entry
+
+
+def test_sorted_adapters_argument_checks_without_gpu():
+    """Early returns and argument errors of the sorted-output adapters are decided on the host
+    before any device work."""
+    L = G.lib()
+    X = np.zeros((2, 3))
+    dist = np.zeros(4)
+    ids = np.zeros(4, dtype=np.int64)
+    cl = ctypes.c_long
+    rc = L.gsknn_direct_kquery_d(G._p(X), G._p(X), cl(2), cl(0), cl(2), cl(3), G._p(dist),
+                                 G._p(ids))
+    assert rc == G.EARLY_RETURN == G.last_error()[0]
+    rc = L.gsknn_direct_kquery_d(G._p(X), G._p(X), cl(2), cl(-1), cl(2), cl(3), G._p(dist),
+                                 G._p(ids))
+    assert rc == 2
+    vp, ci = ctypes.c_void_p, ctypes.c_int
+    L.gsknn_heap_sort_d_device.argtypes = [vp, vp, ci, ci, ci, vp]
+    assert L.gsknn_heap_sort_d_device(None, None, 0, 4, 4, None) == G.EARLY_RETURN
+    assert L.gsknn_heap_sort_d_device(None, None, 3, 4, 4, None) == 2
+    d = np.zeros(8)
+    i = np.zeros(8, dtype=np.int32)
+    assert L.gsknn_heap_sort_d_device(G._p(d), G._p(i), 1, 8, 4, None) == 2  # ldk < k
+    assert L.gsknn_heap_sort_d_device(G._p(d), G._p(i), 1, 600, 600, None) == 5
+    assert "k <= 512" in G.last_error()[1]

@@ -116,3 +116,23 @@ def test_config1_full_size(oracle, golden):
         assert not bad
         Ds, _ = sorted_rows(Dg, Ig)
         assert np.max(np.abs(Ds - De) / np.maximum(De, 1e-300)) <= 1e-12
+
+
+@pytest.mark.parametrize("case", ["ref_d_basic", "ref_s_basic", "ref_d_ties", "ref_s_ties",
+                                  "ref_d_few", "ref_d_odd"])
+def test_heap_pop_oracle_on_reference_heaps(oracle, golden, case):
+    """The oracle's pop loop (dgsrnn_directKQuery.cpp:112-124) over heap rows the reference
+    library wrote: every row comes out ascending and holds the row's (distance, id) pairs; on
+    rows without equal distances it is the (distance, id) sort of the row."""
+    g = golden(case)
+    D, I = g["Dout"], g["Iout"]
+    Dp, Ip = oracle.heap_pop_rows(D, I)
+    assert np.all(np.diff(Dp, axis=1) >= 0)
+    Ds, Is = sorted_rows(D, I)
+    Dq, Iq = sorted_rows(Dp, Ip.astype(np.int32))
+    assert np.array_equal(Dq, Ds) and np.array_equal(Iq, Is)
+    distinct = np.array([np.unique(r).size == r.size for r in D])
+    assert np.array_equal(Dp[distinct], Ds[distinct])
+    assert np.array_equal(Ip[distinct], Is[distinct].astype(np.int64))
+    if case.endswith("ties"):
+        assert not distinct.all()
