@@ -93,6 +93,9 @@ def parse():
     ap.add_argument("--serve-refs", type=int, default=1 << 22,
                     help="resident reference points of the serving workload")
     ap.add_argument("--serve-requests", type=int, default=400)
+    ap.add_argument("--serve-slice", type=int, default=0,
+                    help="rows per serving batch (0: the engine's default, ~3 ms of work)")
+    ap.add_argument("--serve-slots", type=int, default=2, help="serving stream slots")
     ap.add_argument("--serve-mode", default="auto", choices=list(MODE_NAMES.values()),
                     help="arithmetic of the serving engine (a tensor-core mode or auto)")
     ap.add_argument("--serve-rate", type=float, default=150.0,
@@ -586,7 +589,7 @@ def serving_form(L, G, W, dev, args):
     qs = [W.uniform_table(5000 + i, int(ms[i]), d).astype(np.float32) for i in range(n)]
     serve_mode = {v: k for k, v in MODE_NAMES.items()}[args.serve_mode]
     srv = SV.Server(Rd, R2d, mode=serve_mode, max_batch_queries=8192, max_k=64,
-                    heap_budget=2 << 30, slots=3)
+                    heap_budget=2 << 30, slots=args.serve_slots, slice_rows=args.serve_slice)
     for m_w in (1, 128, 4096):  # warm-up: module loads, first launches of every kernel
         rid = srv.submit(W.uniform_table(99, m_w, d).astype(np.float32), 64)
         srv.wait(rid)
@@ -606,7 +609,7 @@ def serving_form(L, G, W, dev, args):
                     time.sleep(dt)
                 ids[i] = srv.submit(qs[i], int(ks[i]))
 
-        lat, queue, rows = [], [], []
+        lat, queue, rows, first = [], [], [], []
         t0 = time.perf_counter()
         th = threading.Thread(target=arrivals)
         th.start()
@@ -618,10 +621,19 @@ def serving_form(L, G, W, dev, args):
             lat.append(st["total_ms"])
             queue.append(st["queue_ms"])
             rows.append(st["batch_rows"])
+            first.append(st["batch"])
             srv.release(ids[i])
         t1 = time.perf_counter()
         th.join()
-        return np.asarray(lat), np.asarray(queue), np.asarray(rows), t1 - t0
+        return (np.asarray(lat), np.asarray(queue), np.asarray(rows), np.asarray(first),
+                t1 - t0)
+
+    def slowest(lat, queue, rows, first, mm, kk, count=5):
+        """The slowest requests: arrival index, rows, k, latency, queue time, first batch."""
+        order = np.argsort(-lat)[:count]
+        return [{"i": int(i), "m": int(mm[i]), "k": int(kk[i]), "ms": round(float(lat[i]), 2),
+                 "queue_ms": round(float(queue[i]), 2), "first_batch_rows": int(rows[i]),
+                 "first_batch": int(first[i])} for i in order]
 
     def summary(lat, queue, mm):
         big = lat[mm >= 2048]
@@ -632,9 +644,9 @@ def serving_form(L, G, W, dev, args):
                 "queue_p50": float(np.percentile(queue, 50)),
                 "queue_p99": float(np.percentile(queue, 99))}
 
-    lat, queue, rows, wall = run_stream(n, args.serve_rate, 56)
+    lat, queue, rows, first, wall = run_stream(n, args.serve_rate, 56)
     n_light = max(1, n // 2)
-    lat_l, queue_l, rows_l, wall_l = run_stream(n_light, args.serve_rate / 3.0, 57)
+    lat_l, queue_l, rows_l, first_l, wall_l = run_stream(n_light, args.serve_rate / 3.0, 57)
     srv.close()
     evals = float(ms.sum()) * nref
     res = {
@@ -646,9 +658,13 @@ def serving_form(L, G, W, dev, args):
         "latency_ms": summary(lat, queue, ms),
         "value": evals / wall, "unit": "distance-evals/s",
         "wall_s": wall, "mean_batch_rows": float(np.mean(rows)),
+        "slice_rows": srv.slice_rows, "slots": args.serve_slots,
+        "slowest": slowest(lat, queue, rows, first, ms, ks),
         "light_load": {"requests": n_light, "rate_per_s": args.serve_rate / 3.0,
                        "latency_ms": summary(lat_l, queue_l, ms[:n_light]),
-                       "mean_batch_rows": float(np.mean(rows_l))},
+                       "mean_batch_rows": float(np.mean(rows_l)),
+                       "slowest": slowest(lat_l, queue_l, rows_l, first_l, ms[:n_light],
+                                          ks[:n_light])},
         "p99_target_ms": 5.0,
     }
     # the same requests one at a time through the per-call entry point: plain FP32 CUDA-core

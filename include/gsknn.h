@@ -273,11 +273,15 @@ void gsknn_batch_forget_tuning(void);
  * on the device until the request is released.
  *
  * A dispatcher thread admits queued requests in arrival order while their heaps (m*k*8 bytes)
- * fit `heap_budget` bytes of device memory, packs admitted requests into batches of at most
- * max_batch_queries rows and runs each batch on one of `slots` streams: requests that arrive
- * while a batch is on the GPU start in the next free slot (continuous batching). A request's
- * result does not depend on its batch. Released requests return their heap memory to the
- * budget; requests that are never released keep it, and later requests then wait. */
+ * fit `heap_budget` bytes of device memory, packs admitted requests into batches and runs each
+ * batch on one of `slots` streams: requests that arrive while a batch is on the GPU start in
+ * the next free slot (continuous batching). A batch holds at most a slice of rows (a multiple
+ * of 128, at most max_batch_queries), by default sized to about 3 ms of tensor work against
+ * this reference set. A request of more rows runs as pieces over several batches, so m is
+ * limited only by the heap budget. Whole requests that fit are packed first, and the oldest
+ * larger request gets at least half of every batch. A request's result does not depend on its
+ * batch or its pieces. Released requests return their heap memory to the budget; requests that
+ * are never released keep it, and later requests then wait. */
 typedef struct gsknn_serve_s gsknn_serve_t;
 gsknn_serve_t *gsknn_serve_create(const float *R, const float *R2, int nref, int d, int mode,
                                   int max_batch_queries, int max_k, size_t heap_budget,
@@ -295,6 +299,9 @@ int gsknn_serve_fetch(gsknn_serve_t *eng, long long id, float *D, int *I);
 int gsknn_serve_stats(gsknn_serve_t *eng, long long id, double *queue_ms, double *total_ms,
                       int *batch, int *batch_rows);
 int gsknn_serve_release(gsknn_serve_t *eng, long long id);
+/* Sets the rows per batch (rounded up to a multiple of 128, at most max_batch_queries; rows <= 0
+ * restores the default) and returns the value in effect; applies to batches formed afterwards. */
+int gsknn_serve_set_slice(gsknn_serve_t *eng, int rows);
 /* While paused (nonzero) the dispatcher starts no new batch; requests still queue. Running
  * batches finish. Resuming dispatches everything queued in arrival order. */
 int gsknn_serve_pause(gsknn_serve_t *eng, int paused);

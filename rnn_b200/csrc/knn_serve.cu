@@ -5,14 +5,24 @@
 //     bound statistics, tc_cand_prepare) and stays resident;
 //   * gsknn_serve_submit() queues a request (m query rows copied from the caller, a k);
 //   * a dispatcher thread admits queued requests in arrival order while their result heaps fit
-//     the heap arena (the HBM budget), packs admitted requests into batches of at most
-//     `max_batch_queries` rows, and launches each batch on a free stream slot, so batches formed
-//     from later arrivals run while earlier ones are still on the GPU (continuous batching);
+//     the heap arena (the HBM budget) and launches batches on free stream slots, so batches
+//     formed from later arrivals run while earlier ones are still on the GPU (continuous
+//     batching);
+//   * a batch holds at most `slice` rows, sized so that one batch is a few milliseconds of
+//     tensor work. The tensor-core kernel keeps one CTA on every SM for the whole batch, so a
+//     small request launched behind a long batch would wait for all of it. Larger requests run
+//     as row pieces over several batches, and whole requests that fit go first, so a small
+//     arrival waits for at most about one slice. The oldest request too large to fit whole
+//     still gets half of every batch, so it cannot starve;
 //   * per batch: one host-to-device copy of the queries, their norms, the tensor-core pass with
 //     the exact FP64 re-rank (tc_run_prepared) at the batch's largest k, and a scatter kernel
 //     that writes each request's k smallest into its own heap, which stays on the device until
 //     the caller releases the request;
-//   * a host function queued behind the batch marks its requests done (no polling).
+//   * a completion thread watches one event per batch (recorded after the batch's last copy)
+//     and marks its requests done. It polls every ~20 us while batches are in flight and
+//     sleeps otherwise. Host functions queued on the stream (cudaLaunchHostFunc) were measured
+//     to run up to 75 ms after the batch's last kernel had ended, a few times per 300 batches,
+//     which set the whole latency tail.
 // Results are the exact FP64 top-k of each query (ties to the lower id), so they are identical
 // whatever a request was batched with.
 #include "gsknn.h"
@@ -23,6 +33,7 @@
 #include <chrono>
 #include <condition_variable>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -47,6 +58,13 @@ __global__ void query_norms(const float *__restrict__ Q, int d, int n, float *__
   }
   for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(FULL_MASK, s, o);
   if (lane == 0) Q2[r] = (float)s;
+}
+
+// GPU wall clock (ns) into *t, for the per-batch trace
+__global__ void stamp(unsigned long long *t) {
+  unsigned long long v;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(v));
+  *t = v;
 }
 
 __global__ void iota(int *__restrict__ a, int n) {
@@ -135,14 +153,22 @@ using Clock = std::chrono::steady_clock;
 struct Request {
   long long id;
   int m, k;
+  int taken = 0;            // rows handed to batches so far
+  int pending = 0;          // pieces launched and not finished
+  bool failed = false;
   std::vector<float> q;     // the caller's query rows
   long long heap_off = -1;  // in the arena
   size_t heap_bytes = 0;
   float *D = nullptr;
   int *I = nullptr;
-  int state = 0;            // 0 queued, 1 admitted, 2 running, 3 done, 4 failed
+  int state = 0;            // 0 queued, 1 admitted, 2 all rows launched, 3 done, 4 failed
   int batch = -1, batch_rows = 0;
   Clock::time_point t_submit, t_launch, t_done;
+};
+
+struct Piece {             // rows [row0, row0 + rows) of a request, inside one batch
+  std::shared_ptr<Request> r;
+  int row0, rows;
 };
 
 struct Slot {
@@ -154,7 +180,11 @@ struct Slot {
   void *ws = nullptr;
   float *h_q = nullptr;       // pinned staging of the batch's queries
   ReqDesc *h_reqs = nullptr;  // pinned staging of the request table
-  std::vector<std::shared_ptr<Request>> batch;
+  std::vector<Piece> batch;
+  int batch_id = -1, batch_rows = 0, batch_k = 0;
+  Clock::time_point t_formed, t_launched;  // for GSKNN_SERVE_TRACE
+  cudaEvent_t done_ev = nullptr;           // recorded behind the batch's status copy
+  bool inflight = false;                   // launched; the completion thread owns it
   gsknn::Engine *eng = nullptr;
   int index = 0;
 };
@@ -164,6 +194,7 @@ struct Slot {
 struct Engine {
   int device;
   int nref, d, mode, max_q, max_k, kp_max, sms, nslots;
+  int slice = 0;  // rows per batch
   size_t heap_budget;
   TcCand C{};
   void *cand_mem = nullptr;
@@ -184,6 +215,10 @@ struct Engine {
   int error = 0;
   char errmsg[256] = {0};
   std::thread dispatcher;
+  std::thread completer;
+  std::condition_variable ccv;  // completion thread: a batch was launched
+  bool trace = false;  // GSKNN_SERVE_TRACE=1: one stderr line per batch
+  serve::Clock::time_point t0 = serve::Clock::now();
 };
 
 }  // namespace gsknn
@@ -193,18 +228,40 @@ namespace gs = gsknn::serve;
 
 static int serr(int code, const char *msg) { return gsknn::set_status(code, "%s", msg); }
 
-// Host function queued behind a batch: marks its requests done and frees the slot.
-static void CUDART_CB batch_done(void *p) {
-  gs::Slot *s = static_cast<gs::Slot *>(p);
+// A piece of r finished (ok or not), called with the lock held: the request is done once all
+// its rows were launched and every piece has finished.
+static void piece_finished(gs::Request &r, bool ok, gs::Clock::time_point now) {
+  r.pending--;
+  if (!ok) r.failed = true;
+  if (r.taken == r.m && r.pending == 0) {
+    r.t_done = now;
+    r.state = r.failed ? 4 : 3;
+  }
+}
+
+// The batch of slot s has finished on the GPU: finish its pieces and free the slot.
+static void batch_done(gs::Slot *s) {
   Engine *E = s->eng;
   const auto now = gs::Clock::now();
   {
     std::lock_guard<std::mutex> lk(E->mu);
+    s->inflight = false;
     int st = 0;
     std::memcpy(&st, s->h_reqs + E->max_q, sizeof(int));  // status copied back by the batch
-    for (auto &r : s->batch) {
-      r->t_done = now;
-      r->state = st == 0 ? 3 : 4;
+    for (auto &pc : s->batch) piece_finished(*pc.r, st == 0, now);
+    if (E->trace) {
+      using ms = std::chrono::duration<double, std::milli>;
+      unsigned long long g[4];
+      std::memcpy(g, reinterpret_cast<const char *>(s->h_reqs + E->max_q) + 8, sizeof(g));
+      std::fprintf(stderr,
+                   "gsknn serve: slot %d batch %d pieces %zu rows %d k %d formed %.3f "
+                   "launched %.3f done %.3f ms | gpu start %.3f prep %.3f tc %.3f scatter %.3f "
+                   "ms\n",
+                   s->index, s->batch_id, s->batch.size(), s->batch_rows, s->batch_k,
+                   ms(s->t_formed - E->t0).count(), ms(s->t_launched - E->t0).count(),
+                   ms(now - E->t0).count(), (double)(g[0] % 1000000000000ull) * 1e-6,
+                   (double)(g[1] - g[0]) * 1e-6, (double)(g[2] - g[1]) * 1e-6,
+                   (double)(g[3] - g[2]) * 1e-6);
     }
     s->batch.clear();
     s->busy = false;
@@ -217,38 +274,88 @@ static void CUDART_CB batch_done(void *p) {
 static cudaError_t launch_batch(Engine *E, gs::Slot &s) {
   using namespace gsknn;
   int rows = 0, kb = 0;
-  const int nreq = (int)s.batch.size();
-  for (int i = 0; i < nreq; i++) {
-    auto &r = s.batch[i];
-    std::memcpy(s.h_q + (size_t)rows * E->d, r->q.data(), (size_t)r->m * E->d * 4);
-    s.h_reqs[i] = {rows, r->m, r->k, 0, r->D, r->I};
-    rows += r->m;
-    kb = std::max(kb, r->k);
+  const int npc = (int)s.batch.size();
+  for (int i = 0; i < npc; i++) {
+    const gs::Piece &pc = s.batch[i];
+    const gs::Request &r = *pc.r;
+    std::memcpy(s.h_q + (size_t)rows * E->d, r.q.data() + (size_t)pc.row0 * E->d,
+                (size_t)pc.rows * E->d * 4);
+    s.h_reqs[i] = {rows, pc.rows, r.k, 0, r.D + (size_t)pc.row0 * r.k,
+                   r.I + (size_t)pc.row0 * r.k};
+    rows += pc.rows;
+    kb = std::max(kb, r.k);
   }
   const TcPlan P = tc_plan(rows, E->nref, E->d, kb, E->mode, E->sms, false, E->sms);
   if (!P.ok || P.bytes > E->ws_bytes) return cudaErrorInvalidValue;
   cudaStream_t st = s.st;
   cudaError_t e = cudaMemcpyAsync(s.Xq, s.h_q, (size_t)rows * E->d * 4, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(s.reqs_d, s.h_reqs, (size_t)nreq * sizeof(gs::ReqDesc),
+    e = cudaMemcpyAsync(s.reqs_d, s.h_reqs, (size_t)npc * sizeof(gs::ReqDesc),
                         cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.status, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
+  unsigned long long *stamps = reinterpret_cast<unsigned long long *>(s.status) + 1;
+  if (E->trace) gs::stamp<<<1, 1, 0, st>>>(stamps + 0);
   gs::query_norms<<<(rows + 7) / 8, 256, 0, st>>>(s.Xq, E->d, rows, s.Xq2);
   const long long n = (long long)rows * kb;
   gs::fill_heap<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(s.Db, s.Ib, n);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  if (E->trace) gs::stamp<<<1, 1, 0, st>>>(stamps + 1);
   e = tc_run_prepared(P, E->C, rows, E->d, kb, s.Xq, s.Xq2, E->max_q, s.qidx, s.Db, s.Ib, kb,
                       s.ws, s.status, nullptr, 0, nullptr, st, nullptr, nullptr);
   if (e != cudaSuccess) return e;
   dim3 blk(32, 8);
-  gs::scatter<<<(rows + 7) / 8, blk, 0, st>>>(s.Db, s.Ib, kb, s.reqs_d, nreq, rows);
+  if (E->trace) gs::stamp<<<1, 1, 0, st>>>(stamps + 2);
+  gs::scatter<<<(rows + 7) / 8, blk, 0, st>>>(s.Db, s.Ib, kb, s.reqs_d, npc, rows);
+  if (E->trace) gs::stamp<<<1, 1, 0, st>>>(stamps + 3);
   e = cudaGetLastError();
+  // the status word (and, when tracing, the four stamps after it) to the slot's host area
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(s.h_reqs + E->max_q, s.status, sizeof(int), cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaLaunchHostFunc(st, batch_done, &s);
+    e = cudaMemcpyAsync(s.h_reqs + E->max_q, s.status, E->trace ? 40 : sizeof(int),
+                        cudaMemcpyDeviceToHost, st);
+  s.t_launched = gs::Clock::now();
+  if (e == cudaSuccess) e = cudaEventRecord(s.done_ev, st);
   return e;
+}
+
+// Fill slot s with the next batch (lock held; the front of the queue is admitted). Whole
+// requests go first-fit in arrival order; if the oldest request is too large to fit whole, half
+// the slice is held for it and it gets a piece of at least that size.
+static void form_batch(Engine *E, gs::Slot &s) {
+  const int cap = E->slice, bid = E->next_batch++;
+  const auto now = gs::Clock::now();
+  auto front = E->queue.front();
+  const int reserve = front->m - front->taken > cap ? cap / 2 : 0;
+  int rows = 0;
+  auto take = [&](const std::shared_ptr<gs::Request> &r, int n) {
+    if (r->taken == 0) {
+      r->batch = bid;
+      r->t_launch = now;
+    }
+    s.batch.push_back({r, r->taken, n});
+    r->taken += n;
+    r->pending++;
+    rows += n;
+  };
+  for (auto &r : E->queue) {
+    if (r->state != 1) break;  // admission is a prefix of the queue
+    const int rem = r->m - r->taken;
+    if (rem <= cap - reserve - rows) take(r, rem);
+  }
+  if (front->taken < front->m && rows < cap) take(front, std::min(front->m - front->taken, cap - rows));
+  for (auto &pc : s.batch)
+    if (pc.r->taken == pc.r->m) pc.r->state = 2;
+  for (auto &pc : s.batch)
+    if (pc.r->batch == bid && pc.row0 == 0) pc.r->batch_rows = rows;
+  s.batch_id = bid;
+  s.batch_rows = rows;
+  s.batch_k = 0;
+  for (auto &pc : s.batch) s.batch_k = std::max(s.batch_k, pc.r->k);
+  s.t_formed = now;
+  E->queue.erase(std::remove_if(E->queue.begin(), E->queue.end(),
+                                [](const std::shared_ptr<gs::Request> &r) { return r->state == 2; }),
+                 E->queue.end());
 }
 
 static void dispatcher_loop(Engine *E) {
@@ -277,37 +384,83 @@ static void dispatcher_loop(Engine *E) {
       return !E->queue.empty() && E->queue.front()->state == 1;
     });
     if (E->stop) return;
-    // batch: admitted requests from the front, up to max_q rows
-    int rows = 0, bid = E->next_batch++;
-    while (!E->queue.empty() && E->queue.front()->state == 1 &&
-           rows + E->queue.front()->m <= E->max_q) {
-      auto r = E->queue.front();
-      E->queue.pop_front();
-      r->state = 2;
-      r->batch = bid;
-      r->t_launch = gs::Clock::now();
-      rows += r->m;
-      slot->batch.push_back(r);
-    }
-    for (auto &r : slot->batch) r->batch_rows = rows;
+    form_batch(E, *slot);
     slot->busy = true;
     lk.unlock();
     cudaSetDevice(dev);
     const cudaError_t e = launch_batch(E, *slot);
-    if (e != cudaSuccess) {
+    if (e == cudaSuccess) {
+      {
+        std::lock_guard<std::mutex> g(E->mu);
+        slot->inflight = true;
+      }
+      E->ccv.notify_one();
+    } else {
       std::lock_guard<std::mutex> g(E->mu);
       E->error = GSKNN_ERR_CUDA;
       std::snprintf(E->errmsg, sizeof(E->errmsg), "serving batch launch failed: %s",
                     cudaGetErrorString(e));
-      for (auto &r : slot->batch) {
-        r->state = 4;
-        r->t_done = gs::Clock::now();
+      const auto now = gs::Clock::now();
+      for (auto &pc : slot->batch) {
+        gs::Request &r = *pc.r;
+        if (r.taken < r.m) {  // no further pieces of a failed request
+          r.taken = r.m;
+          E->queue.erase(std::remove(E->queue.begin(), E->queue.end(), pc.r), E->queue.end());
+        }
+        piece_finished(r, false, now);
       }
       slot->batch.clear();
       slot->busy = false;
       E->done_cv.notify_all();
     }
   }
+}
+
+// Completion thread: polls the events of in-flight batches (cudaEventQuery) every ~20 us while
+// there are any, sleeps on ccv otherwise.
+static void completion_loop(Engine *E) {
+  cudaSetDevice(E->device);
+  std::vector<gs::Slot *> live;
+  while (true) {
+    {
+      std::unique_lock<std::mutex> lk(E->mu);
+      E->ccv.wait(lk, [&] {
+        if (E->stop) return true;
+        for (auto &s : E->slots)
+          if (s.inflight) return true;
+        return false;
+      });
+      if (E->stop) return;
+      live.clear();
+      for (auto &s : E->slots)
+        if (s.inflight) live.push_back(&s);
+    }
+    bool any = false;
+    for (gs::Slot *s : live) {
+      const cudaError_t q = cudaEventQuery(s->done_ev);
+      if (q == cudaErrorNotReady) continue;
+      if (q != cudaSuccess) {  // a failed batch: its status word is not trustworthy
+        std::lock_guard<std::mutex> g(E->mu);
+        E->error = GSKNN_ERR_CUDA;
+        std::snprintf(E->errmsg, sizeof(E->errmsg), "serving batch failed: %s",
+                      cudaGetErrorString(q));
+        int bad = GSKNN_ERR_CUDA;
+        std::memcpy(s->h_reqs + E->max_q, &bad, sizeof(int));
+      }
+      batch_done(s);
+      any = true;
+    }
+    if (!any) std::this_thread::sleep_for(std::chrono::microseconds(20));
+  }
+}
+
+// Rows per batch that keep one batch near 3 ms of tensor work on one B200: the exact forms
+// measured about 1.5e12 evals/s at d = 64 and 8.6e11 at d = 128, i.e. about 3e11 eval-dims per
+// 3 ms. Whole query tiles (128 rows), at least one, at most max_batch_queries.
+static int auto_slice(const Engine *E) {
+  const double rows = 3.0e11 / ((double)E->nref * (double)E->d);
+  int s = (int)(rows / 128.0) * 128;
+  return std::min(E->max_q, std::max(128, s));
 }
 
 extern "C" {
@@ -387,11 +540,11 @@ gsknn_serve_t *gsknn_serve_create(const float *R, const float *R2, int nref, int
          cudaMalloc((void **)&s.Db, q * E->kp_max * 4) == cudaSuccess &&
          cudaMalloc((void **)&s.Ib, q * E->kp_max * 4) == cudaSuccess &&
          cudaMalloc((void **)&s.qidx, q * 4) == cudaSuccess &&
-         cudaMalloc((void **)&s.status, 4) == cudaSuccess &&
+         cudaMalloc((void **)&s.status, 64) == cudaSuccess &&
          cudaMalloc((void **)&s.reqs_d, (q + 1) * sizeof(gs::ReqDesc)) == cudaSuccess &&
          cudaMalloc(&s.ws, E->ws_bytes) == cudaSuccess &&
          cudaHostAlloc((void **)&s.h_q, q * d * 4, cudaHostAllocDefault) == cudaSuccess &&
-         cudaHostAlloc((void **)&s.h_reqs, (q + 1) * sizeof(gs::ReqDesc),
+         cudaHostAlloc((void **)&s.h_reqs, (q + 2) * sizeof(gs::ReqDesc),
                        cudaHostAllocDefault) == cudaSuccess;
     if (!ok) break;
     gs::iota<<<(E->max_q + 255) / 256, 256, 0, s.st>>>(s.qidx, E->max_q);
@@ -404,7 +557,16 @@ gsknn_serve_t *gsknn_serve_create(const float *R, const float *R2, int nref, int
     gsknn_serve_destroy(reinterpret_cast<gsknn_serve_t *>(E.release()));
     return nullptr;
   }
+  E->slice = auto_slice(E.get());
+  E->trace = std::getenv("GSKNN_SERVE_TRACE") != nullptr;
+  for (auto &sl : E->slots)
+    if (cudaEventCreateWithFlags(&sl.done_ev, cudaEventDisableTiming) != cudaSuccess) {
+      serr(GSKNN_ERR_CUDA, "gsknn_serve_create: event creation failed");
+      gsknn_serve_destroy(reinterpret_cast<gsknn_serve_t *>(E.release()));
+      return nullptr;
+    }
   Engine *raw = E.release();
+  raw->completer = std::thread(completion_loop, raw);
   raw->dispatcher = std::thread(dispatcher_loop, raw);
   set_status(GSKNN_OK, nullptr);
   return reinterpret_cast<gsknn_serve_t *>(raw);
@@ -413,9 +575,7 @@ gsknn_serve_t *gsknn_serve_create(const float *R, const float *R2, int nref, int
 long long gsknn_serve_submit(gsknn_serve_t *eng, const float *Q, int m, int k) {
   Engine *E = reinterpret_cast<Engine *>(eng);
   if (!E || !Q || m <= 0 || k <= 0) return serr(GSKNN_ERR_ARG, "gsknn_serve_submit: bad args") * -1LL;
-  if (m > E->max_q || k > E->max_k)
-    return -1LL * serr(GSKNN_ERR_UNSUPPORTED,
-                       "gsknn_serve_submit: m above max_batch_queries or k above max_k");
+  if (k > E->max_k) return -1LL * serr(GSKNN_ERR_UNSUPPORTED, "gsknn_serve_submit: k above max_k");
   const size_t hb = (size_t)m * k * 8;
   if (hb > E->heap_budget)
     return -1LL * serr(GSKNN_ERR_UNSUPPORTED, "gsknn_serve_submit: heap larger than the budget");
@@ -530,6 +690,19 @@ int gsknn_serve_release(gsknn_serve_t *eng, long long id) {
   return GSKNN_OK;
 }
 
+int gsknn_serve_set_slice(gsknn_serve_t *eng, int rows) {
+  Engine *E = reinterpret_cast<Engine *>(eng);
+  if (!E) return -serr(GSKNN_ERR_ARG, "gsknn_serve_set_slice: null engine");
+  int s;
+  {
+    std::lock_guard<std::mutex> lk(E->mu);
+    E->slice = rows <= 0 ? auto_slice(E) : std::min(E->max_q, (rows + 127) / 128 * 128);
+    s = E->slice;
+  }
+  gsknn::set_status(GSKNN_OK, nullptr);
+  return s;
+}
+
 int gsknn_serve_pause(gsknn_serve_t *eng, int paused) {
   Engine *E = reinterpret_cast<Engine *>(eng);
   if (!E) return serr(GSKNN_ERR_ARG, "gsknn_serve_pause: null engine");
@@ -549,9 +722,12 @@ void gsknn_serve_destroy(gsknn_serve_t *eng) {
     E->stop = true;
   }
   E->cv.notify_all();
+  E->ccv.notify_all();
   if (E->dispatcher.joinable()) E->dispatcher.join();
+  if (E->completer.joinable()) E->completer.join();
   for (auto &s : E->slots) {
     if (s.st) cudaStreamSynchronize(s.st);
+    if (s.done_ev) cudaEventDestroy(s.done_ev);
     cudaFree(s.Xq); cudaFree(s.Xq2); cudaFree(s.Db); cudaFree(s.Ib); cudaFree(s.qidx);
     cudaFree(s.status); cudaFree(s.reqs_d); cudaFree(s.ws);
     if (s.h_q) cudaFreeHost(s.h_q);

@@ -17,8 +17,9 @@ from rnn_b200 import gsknn as G
 
 class Server:
     def __init__(self, R, R2, mode: int = 0, max_batch_queries: int = 8192, max_k: int = 64,
-                 heap_budget: int = 1 << 30, slots: int = 3):
-        """R, R2: CUDA tensors (float32 nref x d, float32 nref), kept alive by the server."""
+                 heap_budget: int = 1 << 30, slots: int = 3, slice_rows: int = 0):
+        """R, R2: CUDA tensors (float32 nref x d, float32 nref), kept alive by the server.
+        `slice_rows`: rows per batch (0: sized to a few milliseconds of work)."""
         self._keep = (R, R2)
         self.nref, self.d = R.shape
         L = G.lib()
@@ -35,6 +36,7 @@ class Server:
         L.gsknn_serve_release.argtypes = [vp, ll]
         L.gsknn_serve_destroy.argtypes = [vp]
         L.gsknn_serve_pause.argtypes = [vp, ci]
+        L.gsknn_serve_set_slice.argtypes = [vp, ci]
         self._L = L
         h = L.gsknn_serve_create(R.data_ptr(), R2.data_ptr(), self.nref, self.d, mode,
                                  max_batch_queries, max_k, heap_budget, slots)
@@ -42,6 +44,7 @@ class Server:
             raise G.GsknnError(L.gsknn_last_error(), G.last_error())
         self._h = h
         self._shape = {}
+        self.slice_rows = self.set_slice(slice_rows)
 
     def submit(self, Q: np.ndarray, k: int) -> int:
         Q = np.ascontiguousarray(Q, dtype=np.float32)
@@ -92,6 +95,15 @@ class Server:
         if rc != 0:
             raise G.GsknnError(rc, G.last_error())
         self._shape.pop(rid, None)
+
+    def set_slice(self, rows: int) -> int:
+        """Rows per batch for batches formed from now on (0: the default); returns the value in
+        effect."""
+        s = self._L.gsknn_serve_set_slice(self._h, int(rows))
+        if s <= 0:
+            raise G.GsknnError(-s, G.last_error())
+        self.slice_rows = s
+        return s
 
     def pause(self, paused: bool = True) -> None:
         """Hold (or resume) the start of new batches; requests keep queueing."""

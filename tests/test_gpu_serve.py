@@ -57,7 +57,8 @@ def test_serve_requests_are_exact(oracle, mode):
     R, R2, Rd, R2d = _refs(1000, 30000, 128)
     srv = S.Server(Rd, R2d, mode=mode, max_batch_queries=2048, max_k=64, heap_budget=64 << 20,
                    slots=2)
-    reqs = _requests(1001, 6, 128, [1, 7, 130, 600, 1000, 2048], [8, 16, 64])
+    # 2500 rows: more than a batch holds, served in pieces
+    reqs = _requests(1001, 7, 128, [1, 7, 130, 600, 1000, 2048, 2500], [8, 16, 64])
     ids = [srv.submit(Q, k) for Q, k in reqs]
     for rid, (Q, k) in zip(ids, reqs):
         srv.wait(rid)
@@ -145,7 +146,56 @@ def test_serve_rejects_requests_beyond_its_limits():
     srv = S.Server(Rd, R2d, mode=0, max_batch_queries=256, max_k=16, heap_budget=1 << 20,
                    slots=1)
     with pytest.raises(G.GsknnError):
-        srv.submit(np.zeros((257, 16), np.float32), 8)   # more rows than a batch
+        srv.submit(np.zeros((20000, 16), np.float32), 8)  # heap above the whole budget
     with pytest.raises(G.GsknnError):
         srv.submit(np.zeros((10, 16), np.float32), 32)   # k above max_k
+    srv.close()
+
+
+def test_serve_slices_do_not_change_results():
+    """The same requests with whole batches and with 128-row slices (large requests in up to
+    32 pieces): identical heaps bit for bit."""
+    R, R2, Rd, R2d = _refs(1040, 40000, 64)
+    srv = S.Server(Rd, R2d, mode=0, max_batch_queries=4096, max_k=64, heap_budget=256 << 20,
+                   slots=2)
+    assert srv.slice_rows == 4096  # default for this small reference set: the whole batch
+    reqs = _requests(1041, 9, 64, [1, 130, 900, 2000, 4000, 5000], [8, 16, 64])
+    out = {}
+    for rows in (4096, 128):
+        assert srv.set_slice(rows) == rows
+        srv.pause(True)
+        ids = [srv.submit(Q, k) for Q, k in reqs]
+        srv.pause(False)
+        res = []
+        for rid in ids:
+            srv.wait(rid, timeout=60)
+            res.append(srv.fetch(rid))
+            srv.release(rid)
+        out[rows] = res
+    for (D0, I0), (D1, I1) in zip(out[4096], out[128]):
+        assert np.array_equal(D0, D1) and np.array_equal(I0, I1)
+    assert srv.set_slice(0) == 4096 and srv.set_slice(200) == 256
+    srv.close()
+
+
+def test_serve_small_request_shares_the_first_slice_of_a_large_one():
+    """A large request queued first and a small one behind it: the first batch holds the small
+    request whole and a piece of the large one, so the small one finishes first."""
+    R, R2, Rd, R2d = _refs(1050, 60000, 64)
+    srv = S.Server(Rd, R2d, mode=0, max_batch_queries=4096, max_k=64, heap_budget=256 << 20,
+                   slots=1, slice_rows=512)
+    big = W.uniform_table(1051, 4000, 64).astype(np.float32)
+    small = W.uniform_table(1052, 3, 64).astype(np.float32)
+    srv.pause(True)
+    b = srv.submit(big, 16)
+    a = srv.submit(small, 16)
+    srv.pause(False)
+    srv.wait(a, timeout=60)
+    srv.wait(b, timeout=60)
+    sa, sb = srv.stats(a), srv.stats(b)
+    assert sa["batch"] == sb["batch"]          # both start in the first batch
+    assert sa["batch_rows"] == 512             # 3 rows + a 509-row piece of the large one
+    assert sa["total_ms"] < sb["total_ms"]
+    srv.release(a)
+    srv.release(b)
     srv.close()
