@@ -733,10 +733,15 @@ def e2e_host(L, G, p, beta_h, args):
     for _ in range(steps):
         call()
     t = (time.perf_counter() - t0) / steps
+    # bytes the library moves (gsknn_api.cu knn_host): the index lists, the heaps both ways, and
+    # either the referenced rows alone (gathered on the host, when they cover under 60% of the
+    # row range the lists reach) or that whole range of the table and its norms
     lo = int(min(beta_h.min(), p.alpha.min()))
     hi = int(max(beta_h.max(), p.alpha.max()))
-    rows = hi - lo + 1
-    h2d = rows * D_DIM * 4 + rows * 4 + (nq + N_R) * 4 + 2 * nq * K_NN * 4
+    range_rows = hi - lo + 1
+    n_idx = nq + N_R
+    rows = n_idx if n_idx * 10 < range_rows * 6 else range_rows
+    h2d = rows * (D_DIM + 1) * 4 + n_idx * 4 + 2 * nq * K_NN * 4
     d2h = 2 * nq * K_NN * 4
     return {"value": float(nq) * N_R / t, "unit": "distance-evals/s", "ms_per_step": t * 1e3,
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
