@@ -390,7 +390,7 @@ static int knn_device_tc(int mode, int nq, int nc, int d, int k, const float *Xq
     CU(cudaMemcpyAsync(&nfb, static_cast<char *>(ws) + P.o_fbc, sizeof(int),
                        cudaMemcpyDeviceToHost, st));
     CU(cudaStreamSynchronize(st));
-    const double ctas = (double)P.qtiles * P.S, warps = ctas * 8.0;
+    const double ctas = (double)P.qtiles * P.S, warps = ctas * TC_EPI_WARPS;
     std::fprintf(stderr,
                  "gsknn tc: mode=%d n=%d m=%d d=%d k=%d S=%d N=%d NST=%d: logged/query=%.1f "
                  "inserts/query=%.1f loop-iters/warp=%.1f slow-chunks/warp=%.1f "

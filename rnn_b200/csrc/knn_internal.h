@@ -97,6 +97,11 @@ cudaError_t block_run(const LargePlan &P, int nq, int nc, int d, const T *Xq, co
 typedef void (*TraceHook)(void *ctx, const char *name, bool begin, cudaStream_t st,
                           int nkernels);
 
+// Epilogue warps of the tensor-core kernel: TC_EPI_WARPS / 4 per TMEM lane quarter, each with its
+// own band log per (query, split); the first warp of a quarter keeps the row's heap.
+constexpr int TC_EPI_WARPS = 8;
+constexpr int TC_EPI_PARTS = TC_EPI_WARPS / 4;
+
 struct TcPlan {
   bool ok;
   int fmt, elem, d_pad, nkc, a_terms, b_terms, kp;

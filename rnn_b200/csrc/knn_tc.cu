@@ -39,11 +39,14 @@ namespace tc {
 constexpr int TC_M = 128;            // queries per CTA (TMEM lanes)
 constexpr int CHUNK_BYTES = 128;     // K bytes per TMA box / swizzle atom row
 constexpr int A_CHUNK = TC_M * CHUNK_BYTES;  // 16 KB
-// Warp 0 TMA producer, warp 1 MMA issuer, warps 2-9 epilogue: two warps per TMEM lane quarter,
-// the first of each pair (the heap owner) taking the low half of every tile's columns and the
-// second (log only) the high half.
-constexpr int NEPI = 8;
+// Warp 0 TMA producer, warp 1 MMA issuer, then NEPI epilogue warps: NPART per TMEM lane quarter,
+// part j of a quarter taking the j-th of NPART equal column ranges of every tile. Part 0 keeps
+// the rows' heaps; the other parts log only and take the heap root as their threshold.
+constexpr int NEPI = TC_EPI_WARPS;
+constexpr int NPART = TC_EPI_PARTS;
 constexpr int NTHREADS = 32 * (2 + NEPI);
+// accumulator columns per TMEM wait: 64 (two loads) while the registers allow, else 32
+constexpr int EPI_STEP = NPART <= 2 ? 64 : 32;
 constexpr uint32_t LOG_OVF = 1u << 30;
 // The epilogue frees a TMEM accumulator as soon as its reads have landed, while it still uses
 // the tile's candidate norms; the norms therefore get one slot more than the two accumulators
@@ -468,8 +471,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   } else {
     // ---------------- epilogue: one query row per thread ----------------
     const int lq = warp & 3;            // TMEM lane quarter this warp may access
-    const int half = (warp - 2) >> 2;   // 0: heap owner, low columns; 1: log only, high columns
-    const bool owner = half == 0;
+    const int part = (warp - 2) >> 2;   // column range of the tile; part 0 owns the heap
+    const bool owner = part == 0;
     const int row = lq * 32 + lane;
     const int gq = qt * TC_M + row;
     const bool valid = gq < p.Q;
@@ -509,7 +512,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       s.thr = -Num<float>::inf();
       s.Tv = -Num<float>::inf();
     }
-    const int lslot = 2 * split + half;  // this warp's log among the 2S logs of the query
+    const int lslot = NPART * split + part;  // this warp's log among the NPART*S logs of the query
     uint2 *lg = p.log + ((size_t)lslot * p.Q + (valid ? gq : 0)) * p.logcap;
     // One 32-column chunk: approximate distances, a cheap min-filter, and for the rare chunks
     // with survivors a warp-convergent pass in which every lane with pending candidates handles
@@ -633,31 +636,47 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       const float *cnt = cn_s + c * N;
       const int tile = t_begin + lt;
       const size_t cbase = (size_t)tile * N;
-      // this warp's N/2 columns, 64 at a time (two 32-column chunks per TMEM wait); the
-      // accumulator is freed for the MMA warp once the tile's last loads have landed (the norms
-      // stay in their own slot)
-      const int cb = half * (N / 2), ce = cb + N / 2;
-      for (int c0 = cb; c0 < ce; c0 += 64) {
-        uint32_t ra[32], rb[32];
-        __syncwarp();
-        tmem_ld32(taddr + (uint32_t)c0, ra);
-        tmem_ld32(taddr + (uint32_t)c0 + 32u, rb);
-        tmem_wait_ld();
-        reg_fence32(ra);
-        reg_fence32(rb);
-        if (c0 + 64 >= ce) {
-          tc_fence_before();
+      // this warp's N/NPART columns, EPI_STEP at a time (one or two 32-column chunks per TMEM
+      // wait); the accumulator is freed for the MMA warp once the tile's last loads of every
+      // epilogue warp have landed (the norms stay in their own slot)
+      const int cb = part * (N / NPART), ce = cb + N / NPART;
+      for (int c0 = cb; c0 < ce; c0 += EPI_STEP) {
+        if constexpr (EPI_STEP == 64) {
+          uint32_t ra[32], rb[32];
           __syncwarp();
-          if (lane == 0) mbar_arrive(&tempty[b]);
+          tmem_ld32(taddr + (uint32_t)c0, ra);
+          tmem_ld32(taddr + (uint32_t)c0 + 32u, rb);
+          tmem_wait_ld();
+          reg_fence32(ra);
+          reg_fence32(rb);
+          if (c0 + 64 >= ce) {
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty[b]);
+          }
+          const float ma = fast(ra, cnt, c0);
+          const float mb = fast(rb, cnt, c0 + 32);
+          if (p.dbg && valid) {
+            dbg_write(ra, cbase, c0);
+            dbg_write(rb, cbase, c0 + 32);
+          }
+          if (__any_sync(FULL_MASK, ma <= s.Tv)) slow(ra, cbase, c0, ma);
+          if (__any_sync(FULL_MASK, mb <= s.Tv)) slow(rb, cbase, c0 + 32, mb);
+        } else {
+          uint32_t ra[32];
+          __syncwarp();
+          tmem_ld32(taddr + (uint32_t)c0, ra);
+          tmem_wait_ld();
+          reg_fence32(ra);
+          if (c0 + 32 >= ce) {
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty[b]);
+          }
+          const float ma = fast(ra, cnt, c0);
+          if (p.dbg && valid) dbg_write(ra, cbase, c0);
+          if (__any_sync(FULL_MASK, ma <= s.Tv)) slow(ra, cbase, c0, ma);
         }
-        const float ma = fast(ra, cnt, c0);
-        const float mb = fast(rb, cnt, c0 + 32);
-        if (p.dbg && valid) {
-          dbg_write(ra, cbase, c0);
-          dbg_write(rb, cbase, c0 + 32);
-        }
-        if (__any_sync(FULL_MASK, ma <= s.Tv)) slow(ra, cbase, c0, ma);
-        if (__any_sync(FULL_MASK, mb <= s.Tv)) slow(rb, cbase, c0 + 32, mb);
       }
     }
     if (owner) epi_flush(s, heap, row, p.k, pend, np, ksh);
@@ -1125,10 +1144,10 @@ TcPlan tc_plan(int nq, int nc, int d, int k, int mode, int sms, bool with_cand,
   P.o_pa_lo = P.fmt == 2 ? take((size_t)P.q_pad * P.d_pad * elem) : 0;
   P.o_qn = take((size_t)P.q_pad * 4);
   P.o_qnrm = take((size_t)P.q_pad * 4);
-  // two logs per (query, split): one per epilogue warp of a lane quarter
-  P.o_log = take((size_t)2 * P.S * nq * P.logcap * 8);
-  P.o_logcnt = take((size_t)2 * P.S * nq * 4);
-  P.o_kth = take((size_t)2 * P.S * nq * 4);
+  // NPART logs per (query, split): one per epilogue warp of a lane quarter
+  P.o_log = take((size_t)NPART * P.S * nq * P.logcap * 8);
+  P.o_logcnt = take((size_t)NPART * P.S * nq * 4);
+  P.o_kth = take((size_t)NPART * P.S * nq * 4);
   P.o_kth_shared = take((size_t)nq * 4);
   P.o_margin = take((size_t)nq * 4);
   P.o_fbl = take((size_t)nq * 4);
@@ -1245,7 +1264,7 @@ cudaError_t tc_run_prepared(const TcPlan &P, const TcCand &C, int nq, int d, int
   if (e != cudaSuccess) return e;
 
   RerankParams rp{};
-  rp.Q = nq; rp.k = k; rp.S = 2 * P.S; rp.logcap = P.logcap; rp.d = d;
+  rp.Q = nq; rp.k = k; rp.S = NPART * P.S; rp.logcap = P.logcap; rp.d = d;
   rp.log = tp.log; rp.logcnt = tp.logcnt; rp.kth = tp.kth; rp.margin = tp.margin;
   rp.kth_shared = tp.kth_shared;
   rp.Xq = Xq; rp.Xq2 = Xq2; rp.Xc = C.Xc; rp.Xc2 = C.Xc2; rp.qidx = qidx; rp.cid = C.cid;
