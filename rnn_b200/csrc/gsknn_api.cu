@@ -8,12 +8,15 @@
 #include "knn_internal.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cstdarg>
 #include <cstdint>
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <tuple>
@@ -174,26 +177,73 @@ static cudaError_t pinned_stage(size_t bytes, void **out) {
   return cudaSuccess;
 }
 
-// Rows idx[0..n) of the row-major table X (d per row) and their norms, copied one after another
-// into dst / dst2 by parallel host threads.
-template <typename T>
-static void gather_rows(const T *X, const T *X2, int d, const int *idx, int n, T *dst, T *dst2) {
+static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Host threads of the host-pointer path: one per hardware thread, at most 32.
+static unsigned host_threads() {
   unsigned nt = std::thread::hardware_concurrency();
   if (nt == 0) nt = 1;
-  if (nt > 32) nt = 32;
-  const size_t bytes = (size_t)n * d * sizeof(T);
-  if (bytes < ((size_t)8 << 20)) nt = 1;
+  return nt > 32 ? 32 : nt;
+}
+
+// memcpy of `bytes` split over the host threads (one thread below 4 MiB).
+static void par_copy(void *dst, const void *src, size_t bytes) {
+  unsigned nt = host_threads();
+  if (bytes < ((size_t)4 << 20)) nt = 1;
   auto work = [&](unsigned w) {
-    const int a = (int)((long long)n * w / nt), b = (int)((long long)n * (w + 1) / nt);
-    for (int i = a; i < b; i++) {
-      std::memcpy(dst + (size_t)i * d, X + (size_t)idx[i] * d, (size_t)d * sizeof(T));
-      dst2[i] = X2[idx[i]];
-    }
+    const size_t a = bytes * w / nt, b = bytes * (w + 1) / nt;
+    std::memcpy(static_cast<char *>(dst) + a, static_cast<const char *>(src) + a, b - a);
   };
   std::vector<std::thread> pool;
   for (unsigned w = 1; w < nt; w++) pool.emplace_back(work, w);
   work(0);
   for (auto &t : pool) t.join();
+}
+
+// Rows qidx[0..nq) of Xq, then cidx[0..nc) of Xc, and their norms, gathered by the host threads
+// into pinned hrows / hn and copied to drows / dn on stream st. The rows go in chunks: every
+// thread gathers its part of chunk j, and the calling thread enqueues chunk j's copy as soon as
+// all parts are in, so the copies overlap the gathering of the next chunks. Returns the first
+// copy error.
+template <typename T>
+static cudaError_t gather_rows_to_device(const T *Xq, const T *Xq2, const int *qidx, int nq,
+                                         const T *Xc, const T *Xc2, const int *cidx, int nc,
+                                         int d, T *hrows, T *hn, T *drows, T *dn,
+                                         cudaStream_t st) {
+  const size_t n = (size_t)nq + nc, row_bytes = (size_t)d * sizeof(T);
+  const bool big = n * row_bytes >= ((size_t)8 << 20);
+  const unsigned nt = big ? host_threads() : 1;
+  const int nch = n * row_bytes >= ((size_t)32 << 20) ? 8 : 1;
+  std::unique_ptr<std::atomic<unsigned>[]> done(new std::atomic<unsigned>[nch]);
+  for (int j = 0; j < nch; j++) done[j].store(0);
+  auto part = [&](unsigned w, int j) {
+    const size_t c0 = n * j / nch, c1 = n * (j + 1) / nch;
+    const size_t a = c0 + (c1 - c0) * w / nt, b = c0 + (c1 - c0) * (w + 1) / nt;
+    for (size_t i = a; i < b; i++) {
+      const bool q = i < (size_t)nq;
+      const size_t r = q ? (size_t)qidx[i] : (size_t)cidx[i - nq];
+      std::memcpy(hrows + i * d, (q ? Xq : Xc) + r * d, row_bytes);
+      hn[i] = (q ? Xq2 : Xc2)[r];
+    }
+    done[j].fetch_add(1, std::memory_order_release);
+  };
+  std::vector<std::thread> pool;
+  for (unsigned w = 1; w < nt; w++)
+    pool.emplace_back([&, w] {
+      for (int j = 0; j < nch; j++) part(w, j);
+    });
+  cudaError_t err = cudaSuccess;
+  for (int j = 0; j < nch; j++) {
+    part(0, j);
+    while (done[j].load(std::memory_order_acquire) < nt) std::this_thread::yield();
+    const size_t c0 = n * j / nch, c1 = n * (j + 1) / nch;
+    if (err == cudaSuccess)
+      err = cudaMemcpyAsync(drows + c0 * d, hrows + c0 * d, (c1 - c0) * row_bytes,
+                            cudaMemcpyHostToDevice, st);
+  }
+  for (auto &t : pool) t.join();
+  if (err == cudaSuccess) err = cudaMemcpyAsync(dn, hn, n * sizeof(T), cudaMemcpyHostToDevice, st);
+  return err;
 }
 
 // table[(idx[i] - lo)] = rows[i] (and the norms), one warp per row
@@ -510,6 +560,14 @@ int knn_host(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, const int 
     return set_status(GSKNN_ERR_ARG, "invalid sizes");
   if (!Xq || !Xq2 || !qidx || !Xc || !Xc2 || !cidx || !D || !I)
     return set_status(GSKNN_ERR_ARG, "null pointer argument");
+  // GSKNN_HOST_TRACE=1: one stderr line per call with the host-side phases in milliseconds
+  static const bool host_trace = std::getenv("GSKNN_HOST_TRACE") != nullptr;
+  using hclock = std::chrono::steady_clock;
+  const auto h0 = hclock::now();
+  auto hms = [&](hclock::time_point t) {
+    return std::chrono::duration<double, std::milli>(t - h0).count();
+  };
+  hclock::time_point h_gather = h0, h_copy = h0, h_enq = h0, h_done = h0;
   int qlo, qhi, clo, chi;
   if (!index_range(qidx, nq, &qlo, &qhi) || !index_range(cidx, nc, &clo, &chi))
     return set_status(GSKNN_ERR_INDEX, "negative point index");
@@ -543,20 +601,32 @@ int knn_host(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, const int 
     pct = pqt;
     pcn = pqn;
   }
+  // Pinned staging of this call: the heaps first (both directions go through it, so their
+  // copies run at DMA speed), then, on the sparse path, the gathered rows and their norms. The
+  // heaps' copy to the device overlaps the gathering of the rows.
+  const size_t n = (size_t)nq + nc;
+  const size_t hd_bytes = (size_t)nq * ldD * sizeof(T), hi_bytes = (size_t)nq * ldD * 4;
+  const size_t rows_off = al256(al256(hd_bytes) + hi_bytes);
+  const size_t bytes = rows_off + (sparse ? n * d * sizeof(T) + n * sizeof(T) : 0);
+  void *stage = nullptr;
+  CU(cudaStreamSynchronize(st));  // the staging buffer of the previous call is free
+  CU(pinned_stage(bytes, &stage));
+  T *hD = static_cast<T *>(stage);
+  int *hI = reinterpret_cast<int *>(static_cast<char *>(stage) + al256(hd_bytes));
+  par_copy(hD, D, hd_bytes);
+  par_copy(hI, I, hi_bytes);
+  CU(cudaMemcpyAsync(pD, hD, hd_bytes, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(pI, hI, hi_bytes, cudaMemcpyHostToDevice, st));
   if (sparse) {
-    const size_t n = (size_t)nq + nc;
-    const size_t bytes = n * d * sizeof(T) + n * sizeof(T);
-    void *stage = nullptr, *dg = nullptr;
-    CU(cudaStreamSynchronize(st));  // the staging buffer of the previous call is free
-    CU(pinned_stage(bytes, &stage));
-    CU(scratch(SLOT_HGATHER, bytes, st, &dg));
-    T *hrows = static_cast<T *>(stage);
+    void *dg = nullptr;
+    CU(scratch(SLOT_HGATHER, n * d * sizeof(T) + n * sizeof(T), st, &dg));
+    T *hrows = reinterpret_cast<T *>(static_cast<char *>(stage) + rows_off);
     T *hn = hrows + n * d;
-    gather_rows<T>(Xq, Xq2, d, qidx, nq, hrows, hn);
-    gather_rows<T>(Xc, Xc2, d, cidx, nc, hrows + (size_t)nq * d, hn + nq);
-    CU(cudaMemcpyAsync(dg, stage, bytes, cudaMemcpyHostToDevice, st));
-    const T *grows = static_cast<const T *>(dg);
-    const T *gn = grows + n * d;
+    T *grows = static_cast<T *>(dg);
+    T *gn = grows + n * d;
+    CU(gather_rows_to_device<T>(Xq, Xq2, qidx, nq, Xc, Xc2, cidx, nc, d, hrows, hn, grows, gn,
+                                st));
+    h_gather = hclock::now();
     scatter_rows<T><<<(nq + 7) / 8, 256, 0, st>>>(grows, gn, static_cast<const int *>(pqi), nq,
                                                   d, qlo, static_cast<T *>(pqt),
                                                   static_cast<T *>(pqn));
@@ -579,8 +649,7 @@ int knn_host(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, const int 
   const T *dXc = static_cast<const T *>(pct) - (size_t)clo * d;
   const T *dXc2 = static_cast<const T *>(pcn) - clo;
   int rc = GSKNN_OK;
-  CU(cudaMemcpyAsync(pD, D, (size_t)nq * ldD * sizeof(T), cudaMemcpyHostToDevice, st));
-  CU(cudaMemcpyAsync(pI, I, (size_t)nq * ldD * 4, cudaMemcpyHostToDevice, st));
+  h_copy = hclock::now();
   if (path == 0)
     rc = knn_device<T>(nq, nc, d, k, dXq, dXq2, (long long)qhi + 1, static_cast<int *>(pqi),
                        dXc, dXc2, (long long)chi + 1, static_cast<int *>(pci),
@@ -594,11 +663,21 @@ int knn_host(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, const int 
     cudaStreamSynchronize(st);
     return rc;
   }
+  h_enq = hclock::now();
   rc = device_status(st);
   if (rc != GSKNN_OK) return rc;
-  CU(cudaMemcpyAsync(D, pD, (size_t)nq * ldD * sizeof(T), cudaMemcpyDeviceToHost, st));
-  CU(cudaMemcpyAsync(I, pI, (size_t)nq * ldD * 4, cudaMemcpyDeviceToHost, st));
+  h_done = hclock::now();
+  CU(cudaMemcpyAsync(hD, pD, hd_bytes, cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(hI, pI, hi_bytes, cudaMemcpyDeviceToHost, st));
   CU(cudaStreamSynchronize(st));
+  par_copy(D, hD, hd_bytes);
+  par_copy(I, hI, hi_bytes);
+  if (host_trace)
+    std::fprintf(stderr,
+                 "gsknn host: n=%d m=%d sparse=%d gather %.3f copies-enqueued %.3f "
+                 "kernels-enqueued %.3f device-done %.3f heaps-back %.3f ms\n",
+                 nq, nc, sparse ? 1 : 0, hms(h_gather), hms(h_copy), hms(h_enq), hms(h_done),
+                 hms(hclock::now()));
   return set_status(GSKNN_OK, nullptr);
 }
 
