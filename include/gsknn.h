@@ -65,6 +65,8 @@ struct aux_s {
 typedef struct aux_s aux_t;
 
 /* include/gsknn.h:75-88: a set of m neighbour lists of k entries, row stride ldk.
+ * `type` (KNN_2NORM from heapCreate_* / heapAttach_*) selects the distance of sgsknn / dgsknn /
+ * dgsknn_var3 calls on the heap: set it to KNN_1NORM for the 1-norm (see gsknn_s_device_metric).
  * d = 2 for binary heaps; d = 4 for the 4-ary heaps with a 3-slot header that heapCreate_d
  * builds when k > KNN_VAR_THRES (D = [ro,0,0 | heap], I = [k, filled, ldk | heap]). */
 struct heap_s {
@@ -180,6 +182,22 @@ int gsknn_s_device(int m, int n, int d, int k, const float *XA, const float *XA2
 int gsknn_d_device(int m, int n, int d, int k, const double *XA, const double *XA2,
                    long long nA, const int *alpha, const double *XB, const double *XB2,
                    long long nB, const int *beta, double *D, int *I, int ldD, void *stream);
+
+/* gsknn_s_device / gsknn_d_device with a distance type: KNN_2NORM (the squared 2-norm, as
+ * gsknn_*_device) or KNN_1NORM, the sum over dimensions of |a_p - b_p|. The 1-norm is the
+ * reference's rnn_r_1norm_int_d8x4_row.c kernel (declared by its knn_type enum, include/gsknn.h
+ * :51-55, but never selected by its dispatch). Here it runs on the CUDA cores with an in-order
+ * sum in the input precision, so double results equal the reference kernel's bit for bit (ties
+ * to the lower id). For KNN_1NORM the norm arrays are not read and may be NULL. The same metric
+ * is selected for sgsknn / dgsknn / dgsknn_var3 by a heap_t whose `type` is KNN_1NORM. */
+int gsknn_s_device_metric(int type, int m, int n, int d, int k, const float *XA,
+                          const float *XA2, long long nA, const int *alpha, const float *XB,
+                          const float *XB2, long long nB, const int *beta, float *D, int *I,
+                          int ldD, void *stream);
+int gsknn_d_device_metric(int type, int m, int n, int d, int k, const double *XA,
+                          const double *XA2, long long nA, const int *alpha, const double *XB,
+                          const double *XB2, long long nB, const int *beta, double *D, int *I,
+                          int ldD, void *stream);
 
 /* Synchronises `stream` and returns the device-side status of the last call enqueued on it. */
 int gsknn_stream_status(void *stream);

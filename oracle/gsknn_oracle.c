@@ -345,6 +345,47 @@ static void finish_row(entry_t *h, int cnt, int k, double *Dout, int *Iout) {
 DEFINE_EXACT(oracle_knn_exact_d, double)
 DEFINE_EXACT(oracle_knn_exact_s, float)
 
+/* ------------------------------------------------------------------------------------------
+ * 1-norm kNN (kernels/x86_64/sandybridge/rnn_r_1norm_int_d8x4_row.c: per (query, candidate) the
+ * sum over p, in dimension order, of |a_p - b_p| in the working precision, then max(0, .), then
+ * the heap select): the same sum here, in T, merged with Din/Iin, tie-resolved like
+ * oracle_knn_exact_*, rows ascending.
+ * ---------------------------------------------------------------------------------------- */
+#define DEFINE_EXACT_L1(NAME, T, ABS)                                                       \
+  void NAME(int m, int n, int d, int k, const T *XA, const int *alpha, const T *XB,         \
+            const int *beta, const T *Din, const int *Iin, int ldin, double *Dout,          \
+            int *Iout) {                                                                    \
+    if (n == 0 || k == 0) return;                                                           \
+    int nt = nthreads_for((long)m * n * (d > 0 ? d : 1));                                   \
+    _Pragma("omp parallel num_threads(nt)") {                                               \
+      entry_t *h = (entry_t *)malloc(sizeof(entry_t) * (size_t)k);                          \
+      _Pragma("omp for schedule(dynamic, 4)") for (int j = 0; j < n; j++) {                 \
+        int cnt = 0;                                                                        \
+        const T *b = XB + (size_t)beta[j] * d;                                              \
+        if (Din) {                                                                          \
+          for (int t = 0; t < k; t++) {                                                     \
+            entry_t e = {(double)Din[(size_t)j * ldin + t],                                 \
+                         (uint32_t)Iin[(size_t)j * ldin + t]};                              \
+            ent_push_bounded(h, &cnt, k, e);                                                \
+          }                                                                                 \
+        }                                                                                   \
+        for (int i = 0; i < m; i++) {                                                       \
+          const T *a = XA + (size_t)alpha[i] * d;                                           \
+          T acc = (T)0;                                                                     \
+          for (int p = 0; p < d; p++) acc += ABS(a[p] - b[p]);                              \
+          double c = (double)acc;                                                           \
+          if (c != c) c = INFINITY;                                                         \
+          entry_t e = {c, (uint32_t)alpha[i]};                                              \
+          ent_push_bounded(h, &cnt, k, e);                                                  \
+        }                                                                                   \
+        finish_row(h, cnt, k, Dout + (size_t)j * k, Iout + (size_t)j * k);                  \
+      }                                                                                     \
+      free(h);                                                                              \
+    }                                                                                       \
+  }
+DEFINE_EXACT_L1(oracle_knn_exact_l1_d, double, fabs)
+DEFINE_EXACT_L1(oracle_knn_exact_l1_s, float, fabsf)
+
 void oracle_select_rows_d(int m, int n, int k, const double *C, int ldc, const int *alpha,
                           const double *Din, const int *Iin, int ldin,
                           double *Dout, int *Iout) {

@@ -94,6 +94,16 @@ int oracle_is_maxheap_d(int n, int k, int ld, const double *D);
 int oracle_is_maxheap_s(int n, int k, int ld, const float *D);
 int oracle_is_maxheap4_d(int n, int k, int ld, const double *D, const int *I);
 
+/* 1-norm kNN (rnn_r_1norm_int_d8x4_row.c): candidates alpha of XA against queries beta of XB,
+ * in-order sums of |a_p - b_p| in the input precision, merged with Din/Iin (may be NULL),
+ * (distance, unsigned id) order, rows ascending. */
+void oracle_knn_exact_l1_d(int m, int n, int d, int k, const double *XA, const int *alpha,
+                           const double *XB, const int *beta, const double *Din, const int *Iin,
+                           int ldin, double *Dout, int *Iout);
+void oracle_knn_exact_l1_s(int m, int n, int d, int k, const float *XA, const int *alpha,
+                           const float *XB, const int *beta, const float *Din, const int *Iin,
+                           int ldin, double *Dout, int *Iout);
+
 /* Pops of max-heap rows into ascending lists (frame/old/dgsrnn_directKQuery.cpp:112-124). */
 void oracle_heap_pop_rows_d(int n, int k, int ld, double *D, int *I, double *Dout,
                             long long *Iout);

@@ -100,6 +100,19 @@ class Oracle:
           _p(Iout))
         return Dout, Iout
 
+    def knn_exact_l1(self, k, XA, alpha, XB, beta, Din=None, Iin=None):
+        """Sorted k nearest in the 1-norm (in-order sums in the input precision, lower index
+        wins ties), merged with Din/Iin."""
+        n = beta.size
+        Dout = np.empty((n, k), dtype=np.float64)
+        Iout = np.empty((n, k), dtype=np.int32)
+        f = (self.lib.oracle_knn_exact_l1_d if XA.dtype == np.float64
+             else self.lib.oracle_knn_exact_l1_s)
+        ldin = 0 if Din is None else Din.shape[1]
+        f(_i(alpha.size), _i(n), _i(XA.shape[1]), _i(k), _p(XA), _p(alpha), _p(XB), _p(beta),
+          _p(Din), _p(Iin), _i(ldin), _p(Dout), _p(Iout))
+        return Dout, Iout
+
     def select_rows(self, C, alpha, k, Din=None, Iin=None):
         n, ldc = C.shape
         Dout = np.empty((n, k), dtype=np.float64)

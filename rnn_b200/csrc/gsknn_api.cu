@@ -325,14 +325,16 @@ static void trace_hook(void *, const char *name, bool begin, cudaStream_t st, in
 template <typename T>
 int knn_device_simt(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, long long nrows_q,
                     const int *qidx, const T *Xc, const T *Xc2, long long nrows_c,
-                    const int *cidx, T *D, int *I, int ldD, cudaStream_t st) {
+                    const int *cidx, T *D, int *I, int ldD, cudaStream_t st, int metric = 0) {
   if (nq == 0 || nc == 0 || d == 0 || k == 0)
     return set_status(GSKNN_EARLY_RETURN, "early return: m, n, d or k is 0");
   if (nq < 0 || nc < 0 || d < 0 || k < 0 || ldD < k)
     return set_status(GSKNN_ERR_ARG, "invalid sizes (n=%d m=%d d=%d k=%d ldD=%d)", nq, nc, d,
                       k, ldD);
-  if (!Xq || !Xq2 || !qidx || !Xc || !Xc2 || !cidx || !D || !I)
+  // the 1-norm reads no norms
+  if (!Xq || !qidx || !Xc || !cidx || !D || !I || (metric == 0 && (!Xq2 || !Xc2)))
     return set_status(GSKNN_ERR_ARG, "null pointer argument");
+  if (metric) Xq2 = Xc2 = nullptr;
   const SimtGeom g = simt_geometry<T>(k);
   if (g.kp == 0)
     return set_status(GSKNN_ERR_UNSUPPORTED, "k=%d exceeds the fused kernel's list size", k);
@@ -381,6 +383,7 @@ int knn_device_simt(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, lon
   sa.Apack = Apack; sa.Bpack = Bpack; sa.qn = qn; sa.cn = cn; sa.cid = cid;
   sa.Din = D; sa.ldD = ldD; sa.Q = nq; sa.k = k; sa.nkc = nkc;
   sa.ntiles_r = rtiles; sa.tiles_per_split = tps; sa.partD = partD; sa.partI = partI;
+  sa.metric = metric;
   {
     TraceScope ts("fused_knn_simt", st);
     CU(launch_simt<T>(sa, g.kp, qtiles, S, st));
@@ -474,14 +477,15 @@ static int pick_mode(int nq, int nc, int d, int k) {
 template <typename T>
 int knn_device_large(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, long long nrows_q,
                      const int *qidx, const T *Xc, const T *Xc2, long long nrows_c,
-                     const int *cidx, T *D, int *I, int ldD, int four_ary, cudaStream_t st) {
+                     const int *cidx, T *D, int *I, int ldD, int four_ary, cudaStream_t st,
+                     int metric = 0) {
   if (nq == 0 || nc == 0 || d == 0 || k == 0)
     return set_status(GSKNN_EARLY_RETURN, "early return: m, n, d or k is 0");
   const int need = four_ary ? k + KNN_HEAP_OFFSET : k;
   if (nq < 0 || nc < 0 || d < 0 || k < 0 || ldD < need)
     return set_status(GSKNN_ERR_ARG, "invalid sizes (n=%d m=%d d=%d k=%d ldD=%d)", nq, nc, d,
                       k, ldD);
-  if (!Xq || !Xq2 || !qidx || !Xc || !Xc2 || !cidx || !D || !I)
+  if (!Xq || !qidx || !Xc || !cidx || !D || !I || (metric == 0 && (!Xq2 || !Xc2)))
     return set_status(GSKNN_ERR_ARG, "null pointer argument");
   if (large_select_smem(k, sizeof(T)) > 227 * 1024)
     return set_status(GSKNN_ERR_UNSUPPORTED, "k=%d exceeds the selection kernel (k <= %d)", k,
@@ -496,7 +500,7 @@ int knn_device_large(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, lo
     // two packing launches, then a distance block and a selection per chunk of query rows
     TraceScope ts("select_rows", st, 2 + 2 * ((nq + P.chunk_rows - 1) / P.chunk_rows));
     CU(large_run<T>(P, nq, nc, d, k, Xq, Xq2, nrows_q, qidx, Xc, Xc2, nrows_c, cidx, D, I, ldD,
-                    four_ary, ws, status, st));
+                    four_ary, ws, status, st, metric));
   }
   return set_status(GSKNN_OK, nullptr);
 }
@@ -504,7 +508,14 @@ int knn_device_large(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, lo
 template <typename T>
 int knn_device(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, long long nrows_q,
                const int *qidx, const T *Xc, const T *Xc2, long long nrows_c, const int *cidx,
-               T *D, int *I, int ldD, cudaStream_t st) {
+               T *D, int *I, int ldD, cudaStream_t st, int metric = 0) {
+  if (metric != 0) {  // the 1-norm: CUDA cores only (it is no inner product)
+    if (simt_geometry<T>(k).kp == 0)
+      return knn_device_large<T>(nq, nc, d, k, Xq, Xq2, nrows_q, qidx, Xc, Xc2, nrows_c, cidx,
+                                 D, I, ldD, 0, st, metric);
+    return knn_device_simt<T>(nq, nc, d, k, Xq, Xq2, nrows_q, qidx, Xc, Xc2, nrows_c, cidx, D,
+                              I, ldD, st, metric);
+  }
   if constexpr (std::is_same<T, float>::value) {
     const int mode = pick_mode(nq, nc, d, k);
     if (mode != GSKNN_MODE_FP32)
@@ -552,8 +563,10 @@ static bool index_range(const int *idx, int n, int *lo, int *hi) {
 template <typename T>
 // path: 0 = the default dispatch, 1 = explicit distance block + selection into binary heaps,
 // 2 = the same into 4-ary heaps with the 3-slot header (rows of ldD >= k + 3).
+// metric: 0 = squared 2-norm, 1 = 1-norm (heap_t.type KNN_1NORM).
 int knn_host(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, const int *qidx,
-             const T *Xc, const T *Xc2, const int *cidx, T *D, int *I, int ldD, int path = 0) {
+             const T *Xc, const T *Xc2, const int *cidx, T *D, int *I, int ldD, int path = 0,
+             int metric = 0) {
   if (nq == 0 || nc == 0 || d == 0 || k == 0)
     return set_status(GSKNN_EARLY_RETURN, "early return: m, n, d or k is 0");
   if (nq < 0 || nc < 0 || d < 0 || k < 0 || ldD < (path == 2 ? k + KNN_HEAP_OFFSET : k))
@@ -653,12 +666,12 @@ int knn_host(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, const int 
   if (path == 0)
     rc = knn_device<T>(nq, nc, d, k, dXq, dXq2, (long long)qhi + 1, static_cast<int *>(pqi),
                        dXc, dXc2, (long long)chi + 1, static_cast<int *>(pci),
-                       static_cast<T *>(pD), static_cast<int *>(pI), ldD, st);
+                       static_cast<T *>(pD), static_cast<int *>(pI), ldD, st, metric);
   else
     rc = knn_device_large<T>(nq, nc, d, k, dXq, dXq2, (long long)qhi + 1,
                              static_cast<int *>(pqi), dXc, dXc2, (long long)chi + 1,
                              static_cast<int *>(pci), static_cast<T *>(pD),
-                             static_cast<int *>(pI), ldD, path == 2 ? 1 : 0, st);
+                             static_cast<int *>(pI), ldD, path == 2 ? 1 : 0, st, metric);
   if (rc != GSKNN_OK) {
     cudaStreamSynchronize(st);
     return rc;
@@ -765,6 +778,26 @@ int gsknn_d_device(int m, int n, int d, int k, const double *XA, const double *X
                             (cudaStream_t)stream);
 }
 
+int gsknn_s_device_metric(int type, int m, int n, int d, int k, const float *XA,
+                          const float *XA2, long long nA, const int *alpha, const float *XB,
+                          const float *XB2, long long nB, const int *beta, float *D, int *I,
+                          int ldD, void *stream) {
+  if (type != KNN_2NORM && type != KNN_1NORM)
+    return set_status(GSKNN_ERR_ARG, "type must be KNN_2NORM or KNN_1NORM");
+  return knn_device<float>(n, m, d, k, XB, XB2, nB, beta, XA, XA2, nA, alpha, D, I, ldD,
+                           (cudaStream_t)stream, type == KNN_1NORM ? 1 : 0);
+}
+
+int gsknn_d_device_metric(int type, int m, int n, int d, int k, const double *XA,
+                          const double *XA2, long long nA, const int *alpha, const double *XB,
+                          const double *XB2, long long nB, const int *beta, double *D, int *I,
+                          int ldD, void *stream) {
+  if (type != KNN_2NORM && type != KNN_1NORM)
+    return set_status(GSKNN_ERR_ARG, "type must be KNN_2NORM or KNN_1NORM");
+  return knn_device<double>(n, m, d, k, XB, XB2, nB, beta, XA, XA2, nA, alpha, D, I, ldD,
+                            (cudaStream_t)stream, type == KNN_1NORM ? 1 : 0);
+}
+
 int gsknn_stream_status(void *stream) { return device_status((cudaStream_t)stream); }
 
 int gsknn_tc_distances(int mode, int m, int n, int d, int k, const float *XA, const float *XA2,
@@ -838,7 +871,8 @@ void sgsknn(int m, int n, int k, int r, float *XA, float *XA2, int *alpha, float
     set_status(GSKNN_ERR_ARG, "null heap");
     return;
   }
-  knn_host<float>(n, m, k, r, XB, XB2, beta, XA, XA2, alpha, heap->D_s, heap->I, heap->ldk);
+  knn_host<float>(n, m, k, r, XB, XB2, beta, XA, XA2, alpha, heap->D_s, heap->I, heap->ldk, 0,
+                  heap->type == KNN_1NORM ? 1 : 0);
 }
 
 void dgsknn(int m, int n, int k, int r, double *XA, double *XA2, int *alpha, double *XB,
@@ -851,7 +885,8 @@ void dgsknn(int m, int n, int k, int r, double *XA, double *XA2, int *alpha, dou
     dgsknn_var3(m, n, k, r, XA, XA2, alpha, XB, XB2, beta, heap);
     return;
   }
-  knn_host<double>(n, m, k, r, XB, XB2, beta, XA, XA2, alpha, heap->D, heap->I, heap->ldk);
+  knn_host<double>(n, m, k, r, XB, XB2, beta, XA, XA2, alpha, heap->D, heap->I, heap->ldk, 0,
+                   heap->type == KNN_1NORM ? 1 : 0);
 }
 
 // frame/gsknn.c:597-659. The heap's own layout decides the selection: 4-ary with the header
@@ -863,7 +898,7 @@ void dgsknn_var3(int m, int n, int k, int r, double *XA, double *XA2, int *amap,
     return;
   }
   knn_host<double>(n, m, k, r, XB, XB2, bmap, XA, XA2, amap, heap->D, heap->I, heap->ldk,
-                   heap->d == 4 ? 2 : 1);
+                   heap->d == 4 ? 2 : 1, heap->type == KNN_1NORM ? 1 : 0);
 }
 
 void dgssq2nrm(int m, int n, int k, double *XA, double *XA2, int *amap, double *XB,

@@ -46,6 +46,10 @@ __device__ __forceinline__ double sq_dist(double dot, double cn, double qn) {
   return v < 0.0 ? 0.0 : v;
 }
 
+// |a - b| of the 1-norm distance (the reference's AVX kernel masks the sign bit of a - b)
+__device__ __forceinline__ float abs_diff(float a, float b) { return fabsf(a - b); }
+__device__ __forceinline__ double abs_diff(double a, double b) { return fabs(a - b); }
+
 template <typename T>
 __device__ __forceinline__ void swap_key(T &da, uint32_t &ia, T &db, uint32_t &ib) {
   T td = da; da = db; db = td;

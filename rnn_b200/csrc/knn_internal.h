@@ -42,6 +42,7 @@ struct SimtArgs {
   int ntiles_r, tiles_per_split;
   T *partD;              // [S][Q][k] sorted ascending
   uint32_t *partI;
+  int metric;            // 0: squared 2-norm, 1: 1-norm
 };
 
 template <typename T>
@@ -79,7 +80,8 @@ template <typename T>
 cudaError_t large_run(const LargePlan &P, int nq, int nc, int d, int k, const T *Xq,
                       const T *Xq2, long long nrows_q, const int *qidx, const T *Xc,
                       const T *Xc2, long long nrows_c, const int *cidx, T *D, int *I, int ldD,
-                      int four_ary, void *ws, int *status, cudaStream_t st);
+                      int four_ary, void *ws, int *status, cudaStream_t st,
+                      int metric = 0);  // metric 1: the 1-norm (norms unused)
 template <typename T>
 cudaError_t block_run(const LargePlan &P, int nq, int nc, int d, const T *Xq, const T *Xq2,
                       long long nrows_q, const int *qidx, const T *Xc, const T *Xc2,

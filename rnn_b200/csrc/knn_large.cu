@@ -29,7 +29,9 @@ constexpr int SEL_THREADS = 512;
 // ------------------------------------------------------------------------------------------
 // distance block
 // ------------------------------------------------------------------------------------------
-template <typename T>
+// METRIC 0: squared 2-norm -2<a,b> + |b|^2 + |a|^2 (clamped at 0 when `clamp`); METRIC 1: the
+// 1-norm, sum over p in dimension order of |a_p - b_p|.
+template <typename T, int METRIC>
 __global__ void __launch_bounds__(256) dist_block(const T *__restrict__ Ap, const T *__restrict__ Bp,
                                                   const T *__restrict__ qn,
                                                   const T *__restrict__ cn, int nkc, int Q, int R,
@@ -62,7 +64,10 @@ __global__ void __launch_bounds__(256) dist_block(const T *__restrict__ Ap, cons
 #pragma unroll
       for (int i = 0; i < 4; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        for (int j = 0; j < 4; j++) {
+          if constexpr (METRIC == 1) acc[i][j] += abs_diff(a[i], b[j]);
+          else acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        }
     }
     __syncthreads();
   }
@@ -74,8 +79,11 @@ __global__ void __launch_bounds__(256) dist_block(const T *__restrict__ Ap, cons
     for (int j = 0; j < 4; j++) {
       const int c = ct * LB_T + tx * 4 + j;
       if (c >= R) continue;
-      T v = fma(T(-2), acc[i][j], cn[c]) + qn[q];
-      if (clamp && v < T(0)) v = T(0);
+      T v = acc[i][j];
+      if constexpr (METRIC == 0) {
+        v = fma(T(-2), v, cn[c]) + qn[q];
+        if (clamp && v < T(0)) v = T(0);
+      }
       C[(size_t)(q - q0) * ldc + c] = v;
     }
   }
@@ -291,7 +299,7 @@ template <typename T>
 cudaError_t large_run(const LargePlan &P, int nq, int nc, int d, int k, const T *Xq,
                       const T *Xq2, long long nrows_q, const int *qidx, const T *Xc,
                       const T *Xc2, long long nrows_c, const int *cidx, T *D, int *I, int ldD,
-                      int four_ary, void *ws, int *status, cudaStream_t st) {
+                      int four_ary, void *ws, int *status, cudaStream_t st, int metric) {
   char *base = static_cast<char *>(ws);
   T *Ap = reinterpret_cast<T *>(base + P.o_ap);
   T *Bp = reinterpret_cast<T *>(base + P.o_bp);
@@ -299,10 +307,11 @@ cudaError_t large_run(const LargePlan &P, int nq, int nc, int d, int k, const T 
   T *cn = reinterpret_cast<T *>(base + P.o_cn);
   uint32_t *cid = reinterpret_cast<uint32_t *>(base + P.o_cid);
   T *C = reinterpret_cast<T *>(base + P.o_c);
-  cudaError_t e = launch_pack<T>(Xq, Xq2, d, nrows_q, qidx, nq, LB_T, LB_DK, P.nkc, Ap, qn,
-                                 nullptr, status, st);
+  cudaError_t e = launch_pack<T>(Xq, metric == 1 ? nullptr : Xq2, d, nrows_q, qidx, nq, LB_T,
+                                 LB_DK, P.nkc, Ap, qn, nullptr, status, st);
   if (e == cudaSuccess)
-    e = launch_pack<T>(Xc, Xc2, d, nrows_c, cidx, nc, LB_T, LB_DK, P.nkc, Bp, cn, cid, status, st);
+    e = launch_pack<T>(Xc, metric == 1 ? nullptr : Xc2, d, nrows_c, cidx, nc, LB_T, LB_DK,
+                       P.nkc, Bp, cn, cid, status, st);
   if (e != cudaSuccess) return e;
   if (P.sel_smem > 48 * 1024) {
     e = cudaFuncSetAttribute(select_rows<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -313,8 +322,11 @@ cudaError_t large_run(const LargePlan &P, int nq, int nc, int d, int k, const T 
     const int rows = std::min(P.chunk_rows, nq - q0);
     dim3 grid(P.rtiles, (rows + LB_T - 1) / LB_T);
     // the block covers query tiles [q0 / 64, ...): offset the query panel and norms
-    dist_block<T><<<grid, 256, 0, st>>>(Ap + (size_t)(q0 / LB_T) * P.nkc * LB_DK * LB_T, Bp,
-                                        qn + q0, cn, P.nkc, rows, nc, 0, C, nc, 1);
+    const T *Aq = Ap + (size_t)(q0 / LB_T) * P.nkc * LB_DK * LB_T;
+    if (metric == 1)
+      dist_block<T, 1><<<grid, 256, 0, st>>>(Aq, Bp, qn + q0, cn, P.nkc, rows, nc, 0, C, nc, 1);
+    else
+      dist_block<T, 0><<<grid, 256, 0, st>>>(Aq, Bp, qn + q0, cn, P.nkc, rows, nc, 0, C, nc, 1);
     SelArgs<T> sa{};
     sa.C = C; sa.ldc = nc; sa.cid = cid; sa.m = nc; sa.j0 = q0; sa.D = D; sa.I = I;
     sa.ldD = ldD; sa.k = k; sa.four_ary = four_ary;
@@ -343,7 +355,7 @@ cudaError_t block_run(const LargePlan &P, int nq, int nc, int d, const T *Xq, co
     e = launch_pack<T>(Xc, Xc2, d, nrows_c, cidx, nc, LB_T, LB_DK, P.nkc, Bp, cn, cid, status, st);
   if (e != cudaSuccess) return e;
   dim3 grid(P.rtiles, P.qtiles);
-  dist_block<T><<<grid, 256, 0, st>>>(Ap, Bp, qn, cn, P.nkc, nq, nc, 0, Cout, ldc, 0);
+  dist_block<T, 0><<<grid, 256, 0, st>>>(Ap, Bp, qn, cn, P.nkc, nq, nc, 0, Cout, ldc, 0);
   return cudaGetLastError();
 }
 
@@ -352,7 +364,7 @@ cudaError_t block_run(const LargePlan &P, int nq, int nc, int d, const T *Xq, co
   template cudaError_t large_run<T>(const LargePlan &, int, int, int, int, const T *, const T *, \
                                     long long, const int *, const T *, const T *, long long,    \
                                     const int *, T *, int *, int, int, void *, int *,            \
-                                    cudaStream_t);                                              \
+                                    cudaStream_t, int);                                         \
   template cudaError_t block_run<T>(const LargePlan &, int, int, int, const T *, const T *,     \
                                     long long, const int *, const T *, const T *, long long,    \
                                     const int *, T *, long long, void *, int *, cudaStream_t);

@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(256) pack_panels(
       if (gr < count) {
         const long long row = idx[gr];
         if (row >= 0 && row < nrows) {
-          nv = X2[row];
+          nv = X2 ? X2[row] : T(0);
           id = (uint32_t)row;
         } else {
           atomicExch(status, GSKNN_ERR_INDEX);
@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(256) pack_panels(
 // 2. Fused distance + selection on the CUDA cores: one CTA per (query tile, candidate split);
 //    the tile body is simt_block (knn_simt_body.cuh)
 // ------------------------------------------------------------------------------------------
-template <class C>
+template <class C, int METRIC>
 __global__ void __launch_bounds__(C::NTHR) fused_knn_simt(SimtArgs<typename C::type> a) {
   using T = typename C::type;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(C::NTHR) fused_knn_simt(SimtArgs<typename C::t
   b.outD = a.partD;
   b.outI = a.partI;
   b.out0 = (long long)split * a.Q;
-  simt_block<C>(smem, b);
+  simt_block<C, METRIC>(smem, b);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -167,15 +167,22 @@ cudaError_t launch_pack(const T *X, const T *X2, int d, long long nrows, const i
   return cudaGetLastError();
 }
 
-template <class C>
-static cudaError_t run_simt(const SimtArgs<typename C::type> &a, int qtiles, int S,
-                            cudaStream_t st) {
-  cudaError_t e = cudaFuncSetAttribute(fused_knn_simt<C>,
+template <class C, int METRIC>
+static cudaError_t run_simt_metric(const SimtArgs<typename C::type> &a, int qtiles, int S,
+                                   cudaStream_t st) {
+  cudaError_t e = cudaFuncSetAttribute(fused_knn_simt<C, METRIC>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
   if (e != cudaSuccess) return e;
   dim3 grid(qtiles, S);
-  fused_knn_simt<C><<<grid, C::NTHR, C::SMEM, st>>>(a);
+  fused_knn_simt<C, METRIC><<<grid, C::NTHR, C::SMEM, st>>>(a);
   return cudaGetLastError();
+}
+
+template <class C>
+static cudaError_t run_simt(const SimtArgs<typename C::type> &a, int qtiles, int S,
+                            cudaStream_t st) {
+  return a.metric == METRIC_L1 ? run_simt_metric<C, METRIC_L1>(a, qtiles, S, st)
+                               : run_simt_metric<C, METRIC_L2>(a, qtiles, S, st);
 }
 
 // Tile configurations per (precision, list size). Float: 8x8 per thread, 128 queries x 128

@@ -117,7 +117,14 @@ struct SimtBlock {
   long long out0;
 };
 
-template <class C>
+// Distance of the tile body. L2: squared 2-norm from the dot product and the norms (the
+// reference's rnn_r_int_d8x4_row.c). L1: the sum of |a_p - b_p| over p in dimension order, as
+// the reference's rnn_r_1norm_int_d8x4_row.c accumulates it; the packed candidate norm is used
+// only as the padding flag (0 for a real candidate, NaN past the end).
+constexpr int METRIC_L2 = 0;
+constexpr int METRIC_L1 = 1;
+
+template <class C, int METRIC = METRIC_L2>
 __device__ __forceinline__ void simt_block(unsigned char *smem, const SimtBlock<typename C::type> &a) {
   using T = typename C::type;
   T *Ld = reinterpret_cast<T *>(smem + C::OFF_LD);
@@ -228,7 +235,10 @@ __device__ __forceinline__ void simt_block(unsigned char *smem, const SimtBlock<
 #pragma unroll
       for (int i = 0; i < C::TM; i++)
 #pragma unroll
-        for (int j = 0; j < C::TN; j++) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+        for (int j = 0; j < C::TN; j++) {
+          if constexpr (METRIC == METRIC_L1) acc[i][j] += abs_diff(av[i], bv[j]);
+          else acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+        }
     }
 
     if (c % a.nkc != a.nkc - 1) continue;
@@ -250,7 +260,9 @@ __device__ __forceinline__ void simt_block(unsigned char *smem, const SimtBlock<
     for (int i = 0; i < C::TM; i++)
 #pragma unroll
       for (int j = 0; j < C::TN; j++) {
-        const T dv = sq_dist(acc[i][j], cn_r[j], qn_r[i]);
+        // L1: adding (cn - cn) keeps a real candidate's sum exactly and makes padding NaN
+        const T dv = METRIC == METRIC_L1 ? acc[i][j] + (cn_r[j] - cn_r[j])
+                                         : sq_dist(acc[i][j], cn_r[j], qn_r[i]);
         acc[i][j] = dv;
         if (dv <= thr_r[i]) pend |= 1ull << (i * C::TN + j);
       }

@@ -33,6 +33,7 @@ _lock = threading.Lock()
 
 MODE_AUTO, MODE_FP32, MODE_TF32, MODE_BF16 = 0, 1, 2, 3
 EARLY_RETURN = 1
+KNN_2NORM, KNN_1NORM = 0, 1  # knn_type (include/gsknn.h)
 
 
 class GsknnError(RuntimeError):
@@ -175,6 +176,15 @@ class Heap:
         self.D = numpy.ctypeslib.as_array(src, shape=(self.n, self.ldk))
         self.I = numpy.ctypeslib.as_array(h.I, shape=(self.n, self.ldk))
 
+    @property
+    def type(self) -> int:
+        """heap_t.type: KNN_2NORM (default) or KNN_1NORM, the distance of calls on this heap."""
+        return self.ptr.contents.type
+
+    @type.setter
+    def type(self, t: int) -> None:
+        self.ptr.contents.type = int(t)
+
     def free(self):
         if self.ptr:
             (lib().heapFree_d if self.double else lib().heapFree_s)(self.ptr)
@@ -208,11 +218,13 @@ def dgssq2nrm(XA, XA2, amap, XB, XB2, bmap, ldc=None):
 
 
 # ---- device tensors (torch) -------------------------------------------------------------
-def knn_device(XA, XA2, alpha, XB, XB2, beta, D, I, stream=None, check=True):
+def knn_device(XA, XA2, alpha, XB, XB2, beta, D, I, stream=None, check=True,
+               metric=KNN_2NORM):
     """Fused kNN on CUDA tensors: m = len(alpha) candidates of table XA, n = len(beta) queries
     of table XB; D/I (n, k) heaps on the device, updated in place, asynchronously on `stream`
     (default: torch's current stream). With `check`, synchronises and raises on a device-side
-    error (an index outside its table)."""
+    error (an index outside its table). `metric` KNN_1NORM selects the 1-norm
+    (gsknn_*_device_metric); its norms XA2 / XB2 are not read and may be None."""
     import torch
     L = lib()
     assert D.dim() == 2 and I.shape == D.shape
@@ -220,15 +232,24 @@ def knn_device(XA, XA2, alpha, XB, XB2, beta, D, I, stream=None, check=True):
     d = XA.shape[1]
     dt = XA.dtype
     for t in (XA, XA2, XB, XB2, D):
-        assert t.dtype == dt and t.is_cuda and t.is_contiguous()
+        assert (t is None and metric == KNN_1NORM) or (
+            t.dtype == dt and t.is_cuda and t.is_contiguous())
     for t in (alpha, beta, I):
         assert t.dtype == torch.int32 and t.is_cuda and t.is_contiguous()
     assert beta.numel() == n and XB.shape[1] == d
     st = torch.cuda.current_stream(XA.device) if stream is None else stream
-    f = L.gsknn_s_device if dt == torch.float32 else L.gsknn_d_device
-    rc = f(alpha.numel(), n, d, k, XA.data_ptr(), XA2.data_ptr(), XA.shape[0], alpha.data_ptr(),
-           XB.data_ptr(), XB2.data_ptr(), XB.shape[0], beta.data_ptr(), D.data_ptr(),
-           I.data_ptr(), D.stride(0), st.cuda_stream)
+    ptr = (lambda t: 0 if t is None else t.data_ptr())
+    args = (alpha.numel(), n, d, k, XA.data_ptr(), ptr(XA2), XA.shape[0], alpha.data_ptr(),
+            XB.data_ptr(), ptr(XB2), XB.shape[0], beta.data_ptr(), D.data_ptr(), I.data_ptr(),
+            D.stride(0), st.cuda_stream)
+    if metric == KNN_2NORM:
+        f = L.gsknn_s_device if dt == torch.float32 else L.gsknn_d_device
+        rc = f(*args)
+    else:
+        f = L.gsknn_s_device_metric if dt == torch.float32 else L.gsknn_d_device_metric
+        ll, vp, ci = ctypes.c_longlong, ctypes.c_void_p, ctypes.c_int
+        f.argtypes = [ci, ci, ci, ci, ci, vp, vp, ll, vp, vp, vp, ll, vp, vp, vp, ci, vp]
+        rc = f(metric, *args)
     if rc not in (0, EARLY_RETURN):
         _raise_on_error(False)
     if check:

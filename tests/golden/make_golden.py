@@ -6,7 +6,8 @@ reference library itself, compiled from its sources by oracle/Makefile (`make -C
 on seeded inputs from rnn_b200.workloads. They pin the oracle restatement (oracle/) and give
 the CUDA parity tests fixed expectations. Regenerate with:
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py            # every case
+    make -C oracle ref && python tests/golden/make_golden.py --only l1  # the 1-norm cases
 
 Each case is one .npz with the inputs (or, for the full-size config-1 case, a checksum of the
 regenerated inputs) and the reference outputs.
@@ -164,9 +165,42 @@ def heapselect_case(ref, seed=41):
     save("heapselect", kind="heapselect", **out)
 
 
+def l1_case(name, seed, m, n, d, k, table="uniform"):
+    """The reference's 1-norm micro-kernel (kernels/x86_64/sandybridge/rnn_r_1norm_int_d8x4_row.c)
+    over every 8 x 4 block, driven by oracle/ref_l1_harness.c, into heaps initialised as
+    heapCreate_d does (DBL_MAX, -1): m queries XQ against n candidates XC."""
+    import ctypes
+    lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libref_l1.so"))
+    if table == "grid":  # small integer coordinates: many exact ties
+        XQ = W.randint(seed, m * d, 5).reshape(m, d).astype(np.float64)
+        XC = W.randint(seed + 1, n * d, 5).reshape(n, d).astype(np.float64)
+    else:
+        XQ = W.uniform_table(seed, m, d)
+        XC = W.uniform_table(seed + 1, n, d)
+    D = np.full((m, k), np.finfo(np.float64).max)
+    I = np.full((m, k), -1, dtype=np.int32)
+    Din, Iin = D.copy(), I.copy()
+    vp, ci = ctypes.c_void_p, ctypes.c_int
+    rc = lib.ref_l1_knn(ci(m), ci(n), ci(d), ci(k), vp(XQ.ctypes.data), vp(XC.ctypes.data),
+                        vp(D.ctypes.data), vp(I.ctypes.data))
+    assert rc == 0
+    save(name, kind="l1", k=k, XQ=XQ, XC=XC, Din=Din, Iin=Iin, Dout=D, Iout=I)
+
+
+def l1_cases():
+    l1_case("l1_d_basic", 301, 120, 500, 7, 5)
+    l1_case("l1_d_ties", 302, 90, 300, 3, 8, table="grid")
+    l1_case("l1_d_odd", 303, 31, 257, 33, 7)
+    l1_case("l1_d_few", 304, 20, 5, 6, 16)
+    l1_case("l1_d_dim1", 305, 17, 101, 1, 4)
+
+
 def main():
     if not ReferenceLib.available():
         sys.exit("reference library missing: run `make -C oracle ref` first")
+    if "--only" in sys.argv and sys.argv[sys.argv.index("--only") + 1] == "l1":
+        l1_cases()
+        return
     ref = ReferenceLib()
     ref_oracle_case(ref, "ref_d_basic", 101, 500, 7, 120, 60, 5, np.float64)
     ref_oracle_case(ref, "ref_s_basic", 102, 500, 7, 120, 60, 5, np.float32)
@@ -187,6 +221,7 @@ def main():
     var3_case(ref)
     sq2nrm_case(ref)
     heapselect_case(ref)
+    l1_cases()
 
 
 if __name__ == "__main__":

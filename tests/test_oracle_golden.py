@@ -136,3 +136,32 @@ def test_heap_pop_oracle_on_reference_heaps(oracle, golden, case):
     assert np.array_equal(Ip[distinct], Is[distinct].astype(np.int64))
     if case.endswith("ties"):
         assert not distinct.all()
+
+
+@pytest.mark.parametrize("case", ["l1_d_basic", "l1_d_ties", "l1_d_odd", "l1_d_few",
+                                  "l1_d_dim1"])
+def test_l1_oracle_matches_reference_kernel(oracle, golden, case):
+    """The oracle's 1-norm restatement against the reference's own 1-norm micro-kernel
+    (rnn_r_1norm_int_d8x4_row.c, driven block by block by oracle/ref_l1_harness.c): the same
+    distances bit for bit, and the same index sets except where exact ties at the k-th distance
+    are resolved differently (the reference's heap keeps the later candidate)."""
+    g = golden(case)
+    k, XQ, XC = int(g["k"]), g["XQ"], g["XC"]
+    m, n = XQ.shape[0], XC.shape[0]
+    De, Ie = oracle.knn_exact_l1(k, XC, np.arange(n, dtype=np.int32), XQ,
+                                 np.arange(m, dtype=np.int32), g["Din"], g["Iin"])
+    assert is_maxheap(g["Dout"])
+    Ds, Is = sorted_rows(g["Dout"], g["Iout"])
+    assert np.array_equal(Ds, De)
+    same = np.all(Is == Ie, axis=1)
+    for j in np.nonzero(~same)[0]:
+        kth = De[j, -1]
+        diff = np.setxor1d(Is[j], Ie[j])
+        # every differing id sits exactly at the k-th distance
+        assert np.all(np.isin(diff, Ie[j][De[j] == kth]) | np.isin(diff, Is[j][Ds[j] == kth]))
+        dist = np.abs(XQ[j][None, :] - XC[diff]).sum(axis=1)
+        assert np.all(dist == kth)
+    if case == "l1_d_ties":
+        assert not same.all()
+    if case == "l1_d_few":
+        assert np.all(Is[:, n:] == -1)
