@@ -285,24 +285,23 @@ __device__ __noinline__ int log_compact(uint2 *lg, int cnt, float thr) {
 
 constexpr int PEND = 8;  // heap inserts a lane may defer before the warp flushes them
 
-// Log the candidate and, for heap owners, defer its heap insert into a small register ring
-// (filled through compile-time indices so it stays in registers).
-__device__ __forceinline__ void epi_candidate(EpiState &s, float v, uint32_t id, uint2 *lg,
-                                              int logcap, bool owner, float (&pend)[PEND],
-                                              int &np) {
+// Log the candidate (when `act`) and, for heap owners, defer its heap insert into a small
+// register ring (filled through compile-time indices so it stays in registers). Branch-free:
+// every lane of the warp runs it, with predicates instead of divergent branches.
+__device__ __forceinline__ void epi_candidate(EpiState &s, float v, uint32_t id, bool act,
+                                              uint2 *lg, int logcap, bool owner,
+                                              float (&pend)[PEND], int &np) {
   const float dp = v + s.qn;
-  if (!(dp <= s.thr)) return;
-  s.n_ev++;
-  if (!s.ovf) {
-    if (s.cnt < logcap) lg[s.cnt++] = make_uint2(__float_as_uint(dp), id);
-    else s.ovf = 1;
-  }
-  if (owner && dp < s.root) {
+  const bool take = act && dp <= s.thr;
+  s.n_ev += take ? 1u : 0u;
+  const bool room = s.cnt < logcap;
+  if (take && !s.ovf && room) lg[s.cnt] = make_uint2(__float_as_uint(dp), id);
+  s.cnt += (take && !s.ovf && room) ? 1 : 0;
+  s.ovf |= (take && !room) ? 1 : 0;
+  const bool ins = take && owner && dp < s.root;
 #pragma unroll
-    for (int j = 0; j < PEND; j++)
-      if (j == np) pend[j] = dp;
-    np++;
-  }
+  for (int j = 0; j < PEND; j++) pend[j] = (ins && j == np) ? dp : pend[j];
+  np += ins ? 1 : 0;
 }
 
 // Apply the deferred inserts (all lanes of the warp together, so their sift-downs overlap),
@@ -563,38 +562,36 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           if (s.cnt > p.logcap - 32) s.ovf = 1;
         }
       }
-      uint32_t mask = 0;
-      if (mn <= s.Tv) {
-        // pass mask as an OR tree (depth 5)
-        uint32_t m16[16];
+      // pass mask as an OR tree (depth 5), built by every lane: on this path some lane always
+      // needs it, so a guard would only add a divergent branch
+      uint32_t m16[16];
 #pragma unroll
-        for (int j = 0; j < 16; j++)
-          m16[j] = (__uint_as_float(r[2 * j]) <= s.Tv ? 1u << (2 * j) : 0u) |
-                   (__uint_as_float(r[2 * j + 1]) <= s.Tv ? 1u << (2 * j + 1) : 0u);
+      for (int j = 0; j < 16; j++)
+        m16[j] = (__uint_as_float(r[2 * j]) <= s.Tv ? 1u << (2 * j) : 0u) |
+                 (__uint_as_float(r[2 * j + 1]) <= s.Tv ? 1u << (2 * j + 1) : 0u);
 #pragma unroll
-        for (int w = 8; w >= 1; w >>= 1)
+      for (int w = 8; w >= 1; w >>= 1)
 #pragma unroll
-          for (int j = 0; j < w; j++) m16[j] = m16[2 * j] | m16[2 * j + 1];
-        mask = m16[0];
-      }
+        for (int j = 0; j < w; j++) m16[j] = m16[2 * j] | m16[2 * j + 1];
+      uint32_t mask = m16[0];
       s.n_sc++;
       while (__any_sync(FULL_MASK, mask != 0)) {
         s.n_it++;
-        if (mask) {
-          const int i = __ffs(mask) - 1;
-          mask &= mask - 1;
-          // v[i] for a runtime i: a 5-level select tree on the bits of i
-          float t16[16];
+        // every lane steps: its lowest pending column, or none (act false)
+        const bool act = mask != 0;
+        const int i = (__ffs(mask) - 1) & 31;
+        mask &= mask - 1;
+        // v[i] for a runtime i: a 5-level select tree on the bits of i
+        float t16[16];
 #pragma unroll
-          for (int j = 0; j < 16; j++)
-            t16[j] = __uint_as_float((i & 16) ? r[j + 16] : r[j]);
+        for (int j = 0; j < 16; j++) t16[j] = __uint_as_float((i & 16) ? r[j + 16] : r[j]);
 #pragma unroll
-          for (int w = 8, bit = 8; w >= 1; w >>= 1, bit >>= 1)
+        for (int w = 8, bit = 8; w >= 1; w >>= 1, bit >>= 1)
 #pragma unroll
-            for (int j = 0; j < w; j++) t16[j] = (i & bit) ? t16[j + w] : t16[j];
-          // the log keeps the packed candidate position; the re-rank maps it to the id
-          epi_candidate(s, t16[0], (uint32_t)(cbase + c0 + i), lg, p.logcap, owner, pend, np);
-        }
+          for (int j = 0; j < w; j++) t16[j] = (i & bit) ? t16[j + w] : t16[j];
+        // the log keeps the packed candidate position; the re-rank maps it to the id
+        epi_candidate(s, t16[0], (uint32_t)(cbase + c0 + i), act, lg, p.logcap, owner, pend,
+                      np);
         if (__any_sync(FULL_MASK, np == PEND)) {
           if (owner) epi_flush(s, heap, row, p.k, pend, np, ksh);
         }
