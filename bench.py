@@ -24,6 +24,9 @@ seeded; the reference publishes no dataset for this path.
            points, alpha = beta = leaf, 4 passes merged into one heap): every leaf of a pass in
            one persistent launch replayed from a CUDA graph, tile shape by the autotuner;
            distance evaluations (sum of leaf sizes squared) per second over the 4 passes.
+           `streaming`: the same passes with the point table and heaps in host memory,
+           streamed through the device in groups of 524,288 points (the form for point sets
+           beyond HBM).
 `serving_form`: requests against a resident reference set (4,194,304 points, d = 128,
            U[0,1)): Poisson arrivals, m log-uniform in [1, 4096] queries, k from {8, 16, 64};
            continuous batching inside the library; p50 / p99 latency (submit to result on the
@@ -87,6 +90,8 @@ def parse():
     ap.add_argument("--batch-points", type=int, default=1 << 21,
                     help="points of the batching-form workload (smaller for profiling)")
     ap.add_argument("--batch-passes", type=int, default=4)
+    ap.add_argument("--stream-group", type=int, default=1 << 19,
+                    help="points per group of the streaming measurement (0: skip it)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-form workload")
     ap.add_argument("--serve-only", action="store_true",
                     help="only the serving-form workload (Poisson requests, resident set)")
@@ -561,6 +566,8 @@ def batching_form(L, G, W, dev, peaks, args, threads):
     }
     del Xd, X2d, D, I
     torch.cuda.empty_cache()
+    if args.stream_group > 0:
+        res["streaming"] = streaming_form(B, p, passes, evals, args.stream_group)
     if not args.no_cpu_baseline:
         try:
             res["cpu_baseline"] = batch_cpu_baseline(max(5.0, args.cpu_seconds / 2), threads,
@@ -569,6 +576,36 @@ def batching_form(L, G, W, dev, peaks, args, threads):
         except Exception as e:  # reported, not fatal
             res["cpu_baseline"] = {"error": str(e)[-400:]}
     return res
+
+
+def streaming_form(B, p, passes, evals, group_points):
+    """The same passes with the point table and the heaps in host memory (the streaming form,
+    for point sets beyond HBM): groups of whole leaves of at most `group_points` points go
+    through a device staging table. Host wall time per pass (the call blocks), after one warm-up
+    pass."""
+    D = np.full((p.N, p.k), np.inf, np.float32)
+    I = np.full((p.N, p.k), -1, np.int32)
+    job = B.StreamJob(p.X, p.X2.astype(np.float32), D, I, p.k, group_points=group_points,
+                      leaf_min=p.leaf_min, shape=-1)
+    job.run_pass(passes[0])  # warm-up: staging tuning, graph capture, first touch
+    D.fill(np.inf)
+    I.fill(-1)
+    t0 = time.perf_counter()
+    h2d = d2h = 0.0
+    groups = 0
+    for q in passes:
+        job.run_pass(q)
+        inf = job.info()
+        h2d += inf["h2d_bytes"]
+        d2h += inf["d2h_bytes"]
+        groups += inf["groups"]
+    sec = time.perf_counter() - t0
+    job.close()
+    return {"group_points": group_points, "groups_per_pass": groups / len(passes),
+            "ms_per_pass": sec * 1e3 / len(passes), "value": sum(evals) / sec,
+            "unit": "distance-evals/s",
+            "h2d_bytes_per_pass": h2d / len(passes), "d2h_bytes_per_pass": d2h / len(passes),
+            "note": "point table and heaps in host memory (numpy), host wall clock"}
 
 
 def serving_form(L, G, W, dev, args):

@@ -325,6 +325,42 @@ int gsknn_serve_set_slice(gsknn_serve_t *eng, int rows);
 int gsknn_serve_pause(gsknn_serve_t *eng, int paused);
 void gsknn_serve_destroy(gsknn_serve_t *eng);
 
+/* ---- Streaming form: the batching form for point sets beyond HBM ---------------------------
+ * The point table X / X2 (N x d float, squared norms) and the heap D / I (N rows of stride
+ * ldD >= k, initialised by the caller) are HOST memory: pageable, pinned, or a table mapped from
+ * disk (gsknn_table_open). Each pass takes leaves exactly as gsknn_batch_pass does. The leaves of
+ * a tree partition the points, so every tree is cut into groups of whole leaves of at most
+ * `group_points` points. Each group's rows and heap rows are gathered by host threads, copied
+ * to a device staging table of `group_points` rows, run through the batching pipeline, and
+ * copied back. The next group is gathered while the current one runs. Results equal a resident
+ * gsknn_batch_* job's after the same passes. A leaf larger than group_points is rejected.
+ * Device memory: about group_points * (d + 2k + 2) * 4 bytes plus the staging batch job.
+ * Calls block until the heaps are updated. */
+typedef struct gsknn_stream_s gsknn_stream_t;
+gsknn_stream_t *gsknn_stream_create(int N, int d, int k, const float *X, const float *X2,
+                                    float *D, int *I, int ldD, int group_points, int leaf_min,
+                                    int shape);
+int gsknn_stream_pass(gsknn_stream_t *job, const int *leaf_ptr, const int *leaf_pts,
+                      const int *leaf_tree, int nleaves);
+/* Groups, bytes copied each way and the host time of the last pass. */
+int gsknn_stream_info(const gsknn_stream_t *job, int *groups, double *h2d_bytes,
+                      double *d2h_bytes, double *pass_ms);
+void gsknn_stream_destroy(gsknn_stream_t *job);
+
+/* On-disk point table for the streaming form: a 64-byte header ("GSKNNTB1", version 1, d, N,
+ * offsets), the N x d float32 rows, then their N float32 squared 2-norms, little-endian.
+ * gsknn_table_write writes one (norms from X2, or accumulated in double when X2 is NULL);
+ * gsknn_table_open maps one read-only (NULL and a status if the file is not a valid table);
+ * the row and norm pointers stay valid until gsknn_table_close. */
+typedef struct gsknn_table_s gsknn_table_t;
+int gsknn_table_write(const char *path, const float *X, const float *X2, long long N, int d);
+gsknn_table_t *gsknn_table_open(const char *path);
+long long gsknn_table_rows(const gsknn_table_t *t);
+int gsknn_table_dim(const gsknn_table_t *t);
+const float *gsknn_table_points(const gsknn_table_t *t);
+const float *gsknn_table_norms(const gsknn_table_t *t);
+void gsknn_table_close(gsknn_table_t *t);
+
 /* Randomized projection trees on the host (the caller side of the batching form): `ntrees`
  * trees over the N x d row-major float points X. Each tree first draws leaf sizes uniformly in
  * [leaf_min, leaf_max] (leaf_max >= 2 leaf_min) that sum to N, then splits every node along a

@@ -158,3 +158,111 @@ class BatchJob:
 
 def forget_tuning() -> None:
     G.lib().gsknn_batch_forget_tuning()
+
+
+class StreamJob:
+    """The batching form with the point table and the heaps in HOST memory
+    (`gsknn_stream_create`): numpy arrays X (float32 N x d), X2 (float32 N), D (float32
+    N x ldD), I (int32 N x ldD), or the arrays of a mapped `Table`. Every pass streams groups of
+    whole leaves (at most `group_points` points) through a device staging table and updates D / I
+    in place; the results equal a resident `BatchJob`'s after the same passes."""
+
+    def __init__(self, X, X2, D, I, k: int, group_points: int, leaf_min: int, shape: int = -1):
+        for a, dt in ((X, np.float32), (X2, np.float32), (D, np.float32), (I, np.int32)):
+            assert a.dtype == dt and a.flags["C_CONTIGUOUS"]
+        self._keep = (X, X2, D, I)
+        N, d = X.shape
+        self.N, self.d, self.k = N, d, k
+        L = G.lib()
+        vp, ci = ctypes.c_void_p, ctypes.c_int
+        L.gsknn_stream_create.restype = vp
+        L.gsknn_stream_create.argtypes = [ci, ci, ci, vp, vp, vp, vp, ci, ci, ci, ci]
+        L.gsknn_stream_pass.argtypes = [vp, vp, vp, vp, ci]
+        L.gsknn_stream_info.argtypes = [vp] + [vp] * 4
+        L.gsknn_stream_destroy.argtypes = [vp]
+        self._L = L
+        h = L.gsknn_stream_create(N, d, k, X.ctypes.data, X2.ctypes.data, D.ctypes.data,
+                                  I.ctypes.data, D.shape[1], group_points, leaf_min, shape)
+        if not h:
+            raise G.GsknnError(L.gsknn_last_error(), G.last_error())
+        self._h = h
+
+    def run_pass(self, leaves: Leaves) -> None:
+        """One pass over these leaves; returns when the host heaps are updated."""
+        ptr = np.ascontiguousarray(leaves.ptr, dtype=np.int32)
+        pts = np.ascontiguousarray(leaves.pts, dtype=np.int32)
+        tree = np.ascontiguousarray(leaves.tree, dtype=np.int32)
+        rc = self._L.gsknn_stream_pass(self._h, ptr.ctypes.data, pts.ctypes.data,
+                                       tree.ctypes.data, int(tree.size))
+        if rc != 0:
+            raise G.GsknnError(rc, G.last_error())
+
+    def info(self) -> dict:
+        groups = ctypes.c_int()
+        h2d, d2h, ms = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        self._L.gsknn_stream_info(self._h, ctypes.byref(groups), ctypes.byref(h2d),
+                                  ctypes.byref(d2h), ctypes.byref(ms))
+        return {"groups": groups.value, "h2d_bytes": h2d.value, "d2h_bytes": d2h.value,
+                "pass_ms": ms.value}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._L.gsknn_stream_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def write_table(path: str, X: np.ndarray, X2: np.ndarray | None = None) -> None:
+    """Write the N x d float32 table X (and its squared norms, computed when X2 is None) in the
+    on-disk point-table format (`gsknn_table_write`)."""
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    L = G.lib()
+    L.gsknn_table_write.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_void_p,
+                                    ctypes.c_longlong, ctypes.c_int]
+    x2 = None if X2 is None else np.ascontiguousarray(X2, dtype=np.float32)
+    rc = L.gsknn_table_write(path.encode(), X.ctypes.data,
+                             None if x2 is None else x2.ctypes.data, X.shape[0], X.shape[1])
+    if rc != 0:
+        raise G.GsknnError(rc, G.last_error())
+
+
+class Table:
+    """A point table mapped read-only from disk (`gsknn_table_open`); `X` and `X2` are numpy
+    views of the mapping, valid until `close`."""
+
+    def __init__(self, path: str):
+        L = G.lib()
+        vp = ctypes.c_void_p
+        L.gsknn_table_open.restype = vp
+        L.gsknn_table_open.argtypes = [ctypes.c_char_p]
+        for nm in ("gsknn_table_rows", "gsknn_table_dim", "gsknn_table_points",
+                   "gsknn_table_norms", "gsknn_table_close"):
+            getattr(L, nm).argtypes = [vp]
+        L.gsknn_table_rows.restype = ctypes.c_longlong
+        L.gsknn_table_points.restype = ctypes.POINTER(ctypes.c_float)
+        L.gsknn_table_norms.restype = ctypes.POINTER(ctypes.c_float)
+        self._L = L
+        h = L.gsknn_table_open(path.encode())
+        if not h:
+            raise G.GsknnError(L.gsknn_last_error(), G.last_error())
+        self._h = h
+        self.N, self.d = int(L.gsknn_table_rows(h)), int(L.gsknn_table_dim(h))
+        self.X = np.ctypeslib.as_array(L.gsknn_table_points(h), shape=(self.N, self.d))
+        self.X2 = np.ctypeslib.as_array(L.gsknn_table_norms(h), shape=(self.N,))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self.X = self.X2 = None
+            self._L.gsknn_table_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -64,6 +64,8 @@ __global__ void __launch_bounds__(256) batch_pack(const float *__restrict__ X,
                                                   float *__restrict__ P,
                                                   float *__restrict__ norms,
                                                   uint32_t *__restrict__ ids,
+                                                  uint32_t *__restrict__ rows,
+                                                  const uint32_t *__restrict__ gid,
                                                   int *__restrict__ status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float *s = reinterpret_cast<float *>(smem_raw);  // [DK][BT + 1]
@@ -90,15 +92,17 @@ __global__ void __launch_bounds__(256) batch_pack(const float *__restrict__ X,
         const int gr = tile * BT + r;
         const int row = pidx[gr];
         float nv = Num<float>::nan();
-        uint32_t id = NO_ID;
+        uint32_t id = NO_ID, lr = NO_ID;
         if (row >= 0 && row < N) {
           nv = X2[row];
-          id = (uint32_t)row;
+          lr = (uint32_t)row;
+          id = gid ? gid[row] : lr;
         } else if (row != -1) {
           atomicExch(status, GSKNN_ERR_INDEX);
         }
         norms[gr] = nv;
-        ids[gr] = id;
+        ids[gr] = id;   // the id lists carry (global when gid is given)
+        rows[gr] = lr;  // the heap row of the table (NO_ID: padding)
       }
     }
     __syncthreads();  // the staging tile is reused by the next block
@@ -107,7 +111,8 @@ __global__ void __launch_bounds__(256) batch_pack(const float *__restrict__ X,
 
 struct BatchArgs {
   const float *P, *norms;
-  const uint32_t *ids;
+  const uint32_t *ids;   // candidate ids written to the lists
+  const uint32_t *rows;  // heap rows of the packed rows
   const int4 *items;   // (query tile, first candidate tile, end candidate tile, tree)
   const Meta *meta;
   int *next;           // work-item counter (zeroed before the launch)
@@ -141,7 +146,7 @@ __global__ void __launch_bounds__(C::NTHR) batch_knn_simt(BatchArgs a) {
     b.t_begin = w.y;
     b.t_end = w.z;
     b.nrows = C::BQ;
-    b.rowid = a.ids + (size_t)w.x * C::BQ;
+    b.rowid = a.rows + (size_t)w.x * C::BQ;
     b.row0 = 0;
     b.Din = a.D;
     b.ldD = a.ldD;
@@ -350,7 +355,8 @@ struct BatchJob {
   void *dbuf;
   size_t dbytes;
   float *P, *norms, *outD;
-  uint32_t *ids, *outI;
+  uint32_t *ids, *rows, *outI;
+  const uint32_t *gid;  // global id of each table row (null: the row index itself)
   int *pidx, *stamp, *next, *status;
   int4 *items;
   batch::Meta *meta;
@@ -436,11 +442,13 @@ static cudaError_t enqueue_pass(BatchJob *b, int shape, bool merge) {
   if (e != cudaSuccess) return e;
   const size_t psm = (size_t)gb::DK * (BT + 1) * 4;
   gb::batch_pack<<<b->sms * 8, 256, psm, b->st>>>(
-      b->X, b->X2, b->d, b->N, b->pidx, b->meta, BT, b->nkc, b->P, b->norms, b->ids, b->status);
+      b->X, b->X2, b->d, b->N, b->pidx, b->meta, BT, b->nkc, b->P, b->norms, b->ids, b->rows,
+      b->gid, b->status);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   gb::BatchArgs a{};
-  a.P = b->P; a.norms = b->norms; a.ids = b->ids; a.items = b->items; a.meta = b->meta;
+  a.P = b->P; a.norms = b->norms; a.ids = b->ids; a.rows = b->rows; a.items = b->items;
+  a.meta = b->meta;
   a.next = b->next; a.nkc = b->nkc; a.k = b->k; a.N = b->N; a.D = b->D; a.ldD = b->ldD;
   a.outD = b->outD; a.outI = b->outI; a.stamp = b->stamp;
   e = gb::leaves_any(b->kp, shape, &a, b->sms, b->grid[shape], nullptr, b->st);
@@ -461,6 +469,14 @@ static cudaError_t upload_plan(BatchJob *b, int BT, int ntiles, int nitems) {
   if (e == cudaSuccess) e = cudaEventRecord(b->staged, b->st);
   return e;
 }
+
+namespace gsknn {
+// Rows of the job's table stand for the global points gid[row] (device array, N entries): the
+// lists and the heap carry those ids, while leaves, stamps and heap rows index the table.
+void batch_set_global_ids(void *job, const uint32_t *gid) {
+  reinterpret_cast<BatchJob *>(job)->gid = gid;
+}
+}  // namespace gsknn
 
 extern "C" {
 
@@ -513,7 +529,8 @@ gsknn_batch_t *gsknn_batch_create(int N, int d, int k, const float *X, const flo
   size_t off = 0;
   auto take = [&](size_t n) { size_t o = off; off = (off + n + 255) & ~(size_t)255; return o; };
   const size_t oP = take(rows * (size_t)b->nkc * gb::DK * 4);
-  const size_t oN = take(rows * 4), oId = take(rows * 4), oPidx = take(rows * 4);
+  const size_t oN = take(rows * 4), oId = take(rows * 4), oRow = take(rows * 4),
+               oPidx = take(rows * 4);
   const size_t oOD = take(TN * k * 4), oOI = take(TN * k * 4), oSt = take(TN * 4);
   const size_t oIt = take((size_t)b->max_tiles * sizeof(int4));
   const size_t oMeta = take(sizeof(gb::Meta)), oNext = take(4), oStat = take(4);
@@ -528,6 +545,7 @@ gsknn_batch_t *gsknn_batch_create(int N, int d, int k, const float *X, const flo
   b->P = reinterpret_cast<float *>(base + oP);
   b->norms = reinterpret_cast<float *>(base + oN);
   b->ids = reinterpret_cast<uint32_t *>(base + oId);
+  b->rows = reinterpret_cast<uint32_t *>(base + oRow);
   b->pidx = reinterpret_cast<int *>(base + oPidx);
   b->outD = reinterpret_cast<float *>(base + oOD);
   b->outI = reinterpret_cast<uint32_t *>(base + oOI);

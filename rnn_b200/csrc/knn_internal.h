@@ -104,6 +104,10 @@ typedef void (*TraceHook)(void *ctx, const char *name, bool begin, cudaStream_t 
 constexpr int TC_EPI_WARPS = 8;
 constexpr int TC_EPI_PARTS = TC_EPI_WARPS / 4;
 
+// Batching form: the rows of a job's table (a gsknn_batch_t) stand for global points gid[row]
+// (device array of the job's N rows); lists and heaps then carry global ids (knn_batch.cu).
+void batch_set_global_ids(void *job, const uint32_t *gid);
+
 struct TcPlan {
   bool ok;
   int fmt, elem, d_pad, nkc, a_terms, b_terms, kp;

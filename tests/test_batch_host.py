@@ -96,3 +96,41 @@ def test_allnn_oracle_deduplicates_across_leaves(oracle):
     for row in I1:
         real = row[row >= 0]
         assert np.unique(real).size == real.size
+
+
+def test_point_table_round_trip(tmp_path):
+    """The on-disk table: rows and norms back bit for bit through the read-only mapping; norms
+    computed in double when not given."""
+    X = W.gaussian_mixture_table(33, 3001, 7, dtype=np.float32)
+    X2 = W.sq_norms(X).astype(np.float32)
+    p1, p2 = str(tmp_path / "a.tbl"), str(tmp_path / "b.tbl")
+    B.write_table(p1, X, X2)
+    B.write_table(p2, X)
+    t1, t2 = B.Table(p1), B.Table(p2)
+    assert (t1.N, t1.d) == (3001, 7)
+    assert np.array_equal(t1.X, X) and np.array_equal(t1.X2, X2)
+    assert np.array_equal(t2.X2, X2)  # FP64 sums rounded to float, as sq_norms
+    with open(p1, "rb") as f:
+        head = f.read(64)
+    assert head[:8] == b"GSKNNTB1"
+    assert int.from_bytes(head[16:24], "little") == 3001
+    assert (tmp_path / "a.tbl").stat().st_size == 64 + 3001 * 8 * 4
+    t1.close()
+    t2.close()
+
+
+def test_point_table_rejects_other_files(tmp_path):
+    from rnn_b200 import gsknn as G
+    bad = tmp_path / "bad.tbl"
+    bad.write_bytes(b"NOTATABLE" + bytes(100))
+    with pytest.raises(G.GsknnError):
+        B.Table(str(bad))
+    short = tmp_path / "short.tbl"
+    X = np.ones((10, 4), np.float32)
+    B.write_table(str(short), X)
+    data = short.read_bytes()
+    short.write_bytes(data[:-8])  # truncated norms
+    with pytest.raises(G.GsknnError):
+        B.Table(str(short))
+    with pytest.raises(G.GsknnError):
+        B.Table(str(tmp_path / "missing.tbl"))
