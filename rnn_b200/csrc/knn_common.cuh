@@ -46,6 +46,20 @@ __device__ __forceinline__ double sq_dist(double dot, double cn, double qn) {
   return v < 0.0 ? 0.0 : v;
 }
 
+// Packed FP32 pair FMA of sm_100: (d0, d1) = (a0 * m + c0, a1 * m + c1), each lane rounded to
+// nearest exactly as fmaf, in one instruction.
+__device__ __forceinline__ void fma_pair(float &d0, float &d1, float a0, float a1, float m,
+                                         float c0, float c1) {
+  asm("{\n\t.reg .b64 ra, rm, rc, rd;\n\t"
+      "mov.b64 ra, {%2, %3};\n\t"
+      "mov.b64 rm, {%4, %4};\n\t"
+      "mov.b64 rc, {%5, %6};\n\t"
+      "fma.rn.f32x2 rd, ra, rm, rc;\n\t"
+      "mov.b64 {%0, %1}, rd;\n\t}\n"
+      : "=f"(d0), "=f"(d1)
+      : "f"(a0), "f"(a1), "f"(m), "f"(c0), "f"(c1));
+}
+
 // |a - b| of the 1-norm distance (the reference's AVX kernel masks the sign bit of a - b)
 __device__ __forceinline__ float abs_diff(float a, float b) { return fabsf(a - b); }
 __device__ __forceinline__ double abs_diff(double a, double b) { return fabs(a - b); }

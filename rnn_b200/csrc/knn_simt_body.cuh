@@ -11,6 +11,8 @@
 // the first k entries of every query's list.
 #pragma once
 
+#include <type_traits>
+
 #include "knn_common.cuh"
 #include "knn_internal.h"
 
@@ -233,12 +235,21 @@ __device__ __forceinline__ void simt_block(unsigned char *smem, const SimtBlock<
         for (int u = 0; u < 4; u++) bv[h * 4 + u] = t4[u];
       }
 #pragma unroll
-      for (int i = 0; i < C::TM; i++)
+      for (int i = 0; i < C::TM; i++) {
+        if constexpr (METRIC == METRIC_L2 && std::is_same<T, float>::value) {
+          // two candidates per instruction (packed FP32 FMA, rounded as fmaf)
 #pragma unroll
-        for (int j = 0; j < C::TN; j++) {
-          if constexpr (METRIC == METRIC_L1) acc[i][j] += abs_diff(av[i], bv[j]);
-          else acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+          for (int j = 0; j < C::TN; j += 2)
+            fma_pair(acc[i][j], acc[i][j + 1], bv[j], bv[j + 1], av[i], acc[i][j],
+                     acc[i][j + 1]);
+        } else {
+#pragma unroll
+          for (int j = 0; j < C::TN; j++) {
+            if constexpr (METRIC == METRIC_L1) acc[i][j] += abs_diff(av[i], bv[j]);
+            else acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+          }
         }
+      }
     }
 
     if (c % a.nkc != a.nkc - 1) continue;
