@@ -554,7 +554,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     // Slow part, for a chunk in which some lane has a candidate under its threshold: a
     // warp-convergent pass in which every lane with pending candidates handles one of them per
     // iteration (selected from its registers by index).
-    auto slow = [&](const uint32_t (&r)[32], size_t cbase, int c0, float mn) {
+    auto slow = [&](const uint32_t (&r)[32], size_t cbase, int c0) {
       // a chunk appends at most 32 entries per lane: make room first, all lanes together
       if (__any_sync(FULL_MASK, s.cnt > p.logcap - 32)) {
         if (s.cnt > p.logcap - 32 && !s.ovf) {
@@ -657,8 +657,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             dbg_write(ra, cbase, c0);
             dbg_write(rb, cbase, c0 + 32);
           }
-          if (__any_sync(FULL_MASK, ma <= s.Tv)) slow(ra, cbase, c0, ma);
-          if (__any_sync(FULL_MASK, mb <= s.Tv)) slow(rb, cbase, c0 + 32, mb);
+          if (__any_sync(FULL_MASK, ma <= s.Tv)) slow(ra, cbase, c0);
+          if (__any_sync(FULL_MASK, mb <= s.Tv)) slow(rb, cbase, c0 + 32);
         } else {
           uint32_t ra[32];
           __syncwarp();
@@ -672,7 +672,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           }
           const float ma = fast(ra, cnt, c0);
           if (p.dbg && valid) dbg_write(ra, cbase, c0);
-          if (__any_sync(FULL_MASK, ma <= s.Tv)) slow(ra, cbase, c0, ma);
+          if (__any_sync(FULL_MASK, ma <= s.Tv)) slow(ra, cbase, c0);
         }
       }
     }
