@@ -11,8 +11,9 @@
 //   4. the updated heap rows come back and host threads scatter them into place.
 // Groups of one tree touch disjoint points, so the gather of the next group and the scatter of
 // the previous one overlap the device work of the current one (two pinned staging sets). Trees
-// run one after another, so a point's heap sees the leaves of every tree. The result equals the resident job's after the
-// same passes: the k nearest distinct leaf-mates per point, merged with the incoming heap.
+// run one after another, so a point's heap sees the leaves of every tree. The result equals the
+// resident job's after the same passes: the k nearest distinct leaf-mates per point, merged with
+// the incoming heap.
 #include "gsknn.h"
 #include "knn_internal.h"
 
