@@ -135,6 +135,15 @@ void sgsknn_ref(int m, int n, int k, int r, float *XA, float *XA2, int *alpha, f
 void dgsknn_ref(int m, int n, int k, int r, double *XA, double *XA2, int *alpha, double *XB,
                 double *XB2, int *beta, double *D, int *I);
 
+/* ---- replace frame/gsknn_ref_stl.cpp:81-147 (sgsknn_ref_stl) and 149-214 (dgsknn_ref_stl),
+ *      declared by include/gsknn_ref_stl.hpp: the reference oracle with an STL heap. The same
+ *      GPU path and D/I convention as *_ref; the rows come back as descending binary max-heaps
+ *      (the STL heap keeps its own layout, and on exact ties the earlier candidate). ---- */
+void sgsknn_ref_stl(int m, int n, int k, int r, float *XA, float *XA2, int *alpha, float *XB,
+                    float *XB2, int *beta, float *D, int *I);
+void dgsknn_ref_stl(int m, int n, int k, int r, double *XA, double *XA2, int *alpha,
+                    double *XB, double *XB2, int *beta, double *D, int *I);
+
 /* =====================================================================================
  * Extensions (no counterpart in the reference)
  * ===================================================================================== */

@@ -925,4 +925,15 @@ void dgsknn_ref(int m, int n, int k, int r, double *XA, double *XA2, int *alpha,
   knn_host<double>(n, m, k, r, XB, XB2, beta, XA, XA2, alpha, D, I, r, 1);
 }
 
+// frame/gsknn_ref_stl.cpp:81-214: the same reference algorithm with an STL heap per row.
+void sgsknn_ref_stl(int m, int n, int k, int r, float *XA, float *XA2, int *alpha, float *XB,
+                    float *XB2, int *beta, float *D, int *I) {
+  sgsknn_ref(m, n, k, r, XA, XA2, alpha, XB, XB2, beta, D, I);
+}
+
+void dgsknn_ref_stl(int m, int n, int k, int r, double *XA, double *XA2, int *alpha,
+                    double *XB, double *XB2, int *beta, double *D, int *I) {
+  dgsknn_ref(m, n, k, r, XA, XA2, alpha, XB, XB2, beta, D, I);
+}
+
 }  // extern "C"

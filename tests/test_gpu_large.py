@@ -119,3 +119,31 @@ def test_large_k_fewer_candidates_than_k(oracle):
                               np.full((40, k), -1, dtype=np.int32))
     Ds, Is = sorted_rows(D, I)
     assert np.array_equal(Is, Ie)
+
+
+@pytest.mark.parametrize("case", ["ref_d_stl", "ref_d_basic", "ref_s_basic"])
+def test_ref_stl_entry_points(oracle, golden, case):
+    """sgsknn_ref_stl / dgsknn_ref_stl through the C ABI (frame/gsknn_ref_stl.cpp): the same sets
+    as the exact oracle, and on the STL fixture as the reference's own STL oracle, modulo ties at
+    the k-th distance; rows are valid max-heaps."""
+    import ctypes
+    g = golden(case)
+    X, X2, alpha, beta, k = g["X"], g["X2"], g["alpha"], g["beta"], int(g["k"])
+    D, I = g["Din"].copy(), g["Iin"].copy()
+    L = G.lib()
+    f = L.dgsknn_ref_stl if X.dtype == np.float64 else L.sgsknn_ref_stl
+    ci = ctypes.c_int
+    f(ci(alpha.size), ci(beta.size), ci(X.shape[1]), ci(k), G._p(X), G._p(X2), G._p(alpha),
+      G._p(X), G._p(X2), G._p(beta), G._p(D), G._p(I))
+    assert G.last_error()[0] == 0
+    assert is_maxheap(D)
+    De, Ie = oracle.knn_exact(k, X, X2, alpha, X, X2, beta, g["Din"], g["Iin"])
+    eps = 1e-12 if X.dtype == np.float64 else 4e-6
+    band = eps * np.maximum(1.0, np.abs(De).max(axis=1)) * 16
+    dist_of = lambda j, ids: exact_dists(X, beta[j], ids, X2)  # noqa: E731
+    eq, bad = compare_sets(I, Ie, De, band, dist_of=dist_of)
+    assert not bad, bad[:5]
+    if case == "ref_d_stl":  # the reference STL oracle's own rows
+        Ds, Is = sorted_rows(g["Dout"], g["Iout"])
+        eq, bad = compare_sets(I, Is, Ds, band, dist_of=dist_of)
+        assert not bad, bad[:5]
