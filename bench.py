@@ -155,14 +155,23 @@ def cpu_worker(spec: str) -> None:
             O.gsknn_ref(p.k, p.X, p.X2, p.alpha, p.X, p.X2, beta, D, I)
         return time.perf_counter() - t0
 
-    # size the sample: at least one MC=104 query block per thread (frame/gsknn.c:975-976)
-    q = max(104, min(N_Q, 104 * nthreads // 4))
+    # size the sample: at least one MC=104 query block per thread, since the reference spreads
+    # its query blocks over the threads (frame/gsknn.c:975-976)
+    q = max(104, min(N_Q, 104 * nthreads))
     t = run(q)
     target = cfg["seconds"]
     while t < target / 4 and q < N_Q:
         q = min(N_Q, int(q * max(2.0, target / max(t, 1e-3) * 0.8)))
         t = run(q)
-    out = {"value": q * p.m / t, "seconds": t, "queries": q, "kind": kind, "threads": nthreads}
+    steps, warmup = cfg.get("steps", 1), cfg.get("warmup", 0)
+    times = [t]
+    if steps > 1 or warmup > 0:  # the sizing call is the first warm-up; then W more, K timed
+        for _ in range(max(0, warmup - 1)):
+            run(q)
+        times = [run(q) for _ in range(steps)]
+    t = sum(times)
+    out = {"value": q * p.m * len(times) / t, "seconds": t, "queries": q, "kind": kind,
+           "threads": nthreads, "steps": len(times), "ms_per_step": 1e3 * t / len(times)}
     print("CPUJSON " + json.dumps(out), flush=True)
 
 
@@ -210,8 +219,11 @@ def batch_cpu_baseline(seconds: float, threads: int, points: int) -> dict:
     raise RuntimeError("batch cpu baseline failed:\n" + r.stdout[-2000:] + r.stderr[-2000:])
 
 
-def cpu_baseline(seconds: float, threads: int) -> dict:
-    spec = json.dumps({"threads": threads, "seconds": seconds, "seed": 2})
+def cpu_baseline(seconds: float, threads: int, steps: int = 1, warmup: int = 0) -> dict:
+    """The reference sgsknn on the host cores: a query slice against all references, sized to
+    about `seconds` per call; with steps/warmup, `warmup` untimed calls then `steps` timed ones."""
+    spec = json.dumps({"threads": threads, "seconds": seconds, "seed": 2, "steps": steps,
+                       "warmup": warmup})
     env = dict(os.environ)
     env["CUDA_VISIBLE_DEVICES"] = ""
     r = subprocess.run([sys.executable, os.path.abspath(__file__), "--cpu-worker", spec],
@@ -219,10 +231,11 @@ def cpu_baseline(seconds: float, threads: int) -> dict:
     for line in r.stdout.splitlines():
         if line.startswith("CPUJSON "):
             o = json.loads(line[8:])
+            calls = "one call" if o["steps"] == 1 else f"{o['steps']} timed calls"
             return {"value": o["value"], "unit": "distance-evals/s", "cores": o["threads"],
-                    "kind": o["kind"],
+                    "kind": o["kind"], "ms_per_step": o["ms_per_step"],
                     "sample": (f"{o['queries']} of {N_Q} queries x {N_R} references, k={K_NN}, "
-                               f"one call, {o['seconds']:.1f} s, GSKNN_IC_NT=OMP_NUM_THREADS="
+                               f"{calls}, {o['seconds']:.1f} s, GSKNN_IC_NT=OMP_NUM_THREADS="
                                f"{o['threads']}")}
     raise RuntimeError("cpu baseline failed:\n" + r.stdout[-2000:] + r.stderr[-2000:])
 
@@ -799,10 +812,15 @@ def main():
         # the reference's CPU implementation of the path; rank 0 alone
         if rank != 0:
             return
-        cb = cpu_baseline(max(5.0, args.cpu_seconds), threads)
+        # each step is a bounded sample (a query slice against all references), sized so the
+        # whole --steps K --warmup W run takes about a minute
+        steps, warmup = max(1, args.steps), max(0, args.warmup)
+        per_step = max(0.5, min(args.cpu_seconds, 60.0 / (steps + warmup)))
+        cb = cpu_baseline(per_step, threads, steps=steps, warmup=warmup)
         out = {"impl": "reference", "metric": "distance-evals/s", "value": cb["value"],
-               "unit": "distance-evals/s", "n_gpus": args.gpus, "steps": args.steps,
-               "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+               "unit": "distance-evals/s", "n_gpus": args.gpus, "steps": steps,
+               "warmup": warmup, "ms_per_step": cb["ms_per_step"],
+               "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f32",
                "data": "synthetic (seeded gaussian mixture)",
                "config": {"workload": WORKLOAD, "points": N_POINTS, "d": D_DIM, "queries": N_Q,
