@@ -11,7 +11,7 @@
 #define GSKNN_ERR_ARG 2          // invalid argument
 #define GSKNN_ERR_CUDA 3         // a CUDA runtime call failed
 #define GSKNN_ERR_INDEX 4        // an alpha/beta entry lies outside the point table
-#define GSKNN_ERR_UNSUPPORTED 5  // size outside what this build supports
+#define GSKNN_ERR_UNSUPPORTED 5  // size outside what this library supports
 #define GSKNN_ERR_NOMEM 6        // device memory exhausted
 #define GSKNN_ERR_TIMEOUT 7      // a bounded device-side wait gave up
 
