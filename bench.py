@@ -49,6 +49,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -251,11 +252,11 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{gpu_index}.csv")
+        fd, self.path = tempfile.mkstemp(prefix=f"gsknn_clocks_gpu{gpu_index}_", suffix=".csv")
+        os.close(fd)
 
     def start(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
@@ -287,6 +288,10 @@ class ClockSampler:
             for nm, v in zip(names, parts[5:9]):
                 if v.lower() == "active":
                     reasons.add(nm)
+        try:
+            os.unlink(self.path)
+        except OSError:
+            pass
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": ["unsampled"]}
         loaded = [s for s in sm if s > 0.5 * max(sm)] or sm

@@ -10,7 +10,8 @@
 //                 [rows][d_pad] panel (TMA source), effective norm X2 - 2 mu.x + mu.mu (the
 //                 centred norm, built on the caller's norm) in FP64, centred norm bound, ids;
 //                 running maxima for the bound
-//   tc_knn        warp 0 TMA producer, warp 1 MMA issuer (TMEM owner), warps 2-5 epilogue with
+//   tc_knn        warp 0 TMA producer, warp 1 MMA issuer (TMEM owner), warps 2-9 epilogue (two
+//                 per TMEM lane quarter, each taking half of every tile's columns) with
 //                 one query row per thread: approximate d' = qn' + cn' - 2<q~,c~>, a per-query
 //                 max-heap of the k smallest d' in shared memory (threshold), and a per-query
 //                 log in HBM of every candidate with d' <= k-th + 2E
