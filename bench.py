@@ -134,6 +134,9 @@ def cpu_worker(spec: str) -> None:
     if cfg.get("kind") == "batch":
         batch_cpu_worker(cfg, nthreads)
         return
+    if cfg.get("kind") == "config1":
+        config1_cpu_worker(cfg, nthreads)
+        return
     p = W.config2(seed=cfg["seed"])
     ref_so = os.path.join(ROOT, "oracle", "_ref", "libgsknn_ref.so")
     kind = "reference" if os.path.exists(ref_so) else "port"
@@ -200,6 +203,52 @@ def batch_cpu_worker(cfg, nthreads) -> None:
             break
     print("CPUJSON " + json.dumps({"value": evals / t, "seconds": t, "leaves": n,
                                    "kind": "reference", "threads": nthreads}), flush=True)
+
+
+def config1_cpu_worker(cfg, nthreads) -> None:
+    """The reference's dgsknn (its AVX double path, frame/gsknn.c:1138-1184) on the config-1
+    workload: one step = two merging calls into a heapCreate_d heap, as the GPU leg runs it."""
+    from rnn_b200 import workloads as W
+    from oracle.oracle import ReferenceLib
+    ref_so = os.path.join(ROOT, "oracle", "_ref", "libgsknn_ref.so")
+    p, alpha2 = W.config1(1)
+    R = ReferenceLib(ref_so)
+
+    def step():
+        h = R.heap_create(p.n, p.k, 1.79e308, double=True)
+        t0 = time.perf_counter()
+        R.gsknn(p.k, p.X, p.X2, p.alpha, p.X, p.X2, p.beta, h)
+        R.gsknn(p.k, p.X, p.X2, alpha2, p.X, p.X2, p.beta, h)
+        t = time.perf_counter() - t0
+        R.heap_free(h, double=True)
+        return t
+
+    for _ in range(2):
+        step()
+    times = []
+    while sum(times) < cfg["seconds"] and len(times) < 200:
+        times.append(step())
+    t = sum(times) / len(times)
+    print("CPUJSON " + json.dumps({"value": 2.0 * p.n * p.m / t, "ms_per_step": 1e3 * t,
+                                   "steps": len(times), "kind": "reference",
+                                   "threads": nthreads}), flush=True)
+
+
+def config1_cpu_baseline(seconds: float, threads: int) -> dict:
+    spec = json.dumps({"kind": "config1", "threads": threads, "seconds": seconds})
+    env = dict(os.environ)
+    env["CUDA_VISIBLE_DEVICES"] = ""
+    r = subprocess.run([sys.executable, os.path.abspath(__file__), "--cpu-worker", spec],
+                       capture_output=True, text=True, env=env, timeout=600)
+    for line in r.stdout.splitlines():
+        if line.startswith("CPUJSON "):
+            o = json.loads(line[8:])
+            return {"value": o["value"], "unit": "distance-evals/s", "cores": o["threads"],
+                    "kind": o["kind"], "ms_per_step": o["ms_per_step"],
+                    "sample": (f"reference dgsknn, two merging calls per step into a "
+                               f"heapCreate_d heap, {o['steps']} steps, "
+                               f"GSKNN_IC_NT=OMP_NUM_THREADS={o['threads']}")}
+    raise RuntimeError("config-1 cpu baseline failed:\n" + r.stdout[-2000:] + r.stderr[-2000:])
 
 
 def batch_cpu_baseline(seconds: float, threads: int, points: int) -> dict:
@@ -397,9 +446,13 @@ def roofline(mode_name, prob, trace, peaks, clk):
         bound = "fp32"
     else:
         flops = prob.evals * 2 * d
-        peak = peaks["bf16"] * (0.5 if mode_name == "tf32" else 1.0)
-        src = (f"{peaks['source']} bf16 dense burst peak"
-               + (" x 0.5 (TF32 tensor rate)" if mode_name == "tf32" else ""))
+        if mode_name == "tf32" and peaks.get("tf32_tflops"):
+            peak = peaks["tf32_tflops"]
+            src = "measured TF32 dense GEMM burst rate (peak_probes)"
+        else:
+            peak = peaks["bf16"] * (0.5 if mode_name == "tf32" else 1.0)
+            src = (f"{peaks['source']} bf16 dense burst peak"
+                   + (" x 0.5 (TF32 tensor rate, not probed)" if mode_name == "tf32" else ""))
         bound = "tensor"
     achieved = flops / (kms * 1e-3) / 1e12
     out = {"bound": bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
@@ -410,6 +463,211 @@ def roofline(mode_name, prob, trace, peaks, clk):
         out["note"] = "split BF16 runs 3 MMAs per product; achieved counts the 2d useful flops"
     return out
 
+
+
+# ------------------------------------------------------------------------------------------
+# measured rates that MEASURED_PEAKS.json does not carry
+# ------------------------------------------------------------------------------------------
+def _gemm_tflops(torch, a, b, reps=5):
+    for _ in range(3):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = None
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) * 1e-3
+        best = t if best is None else min(best, t)
+    n = a.shape[0]
+    return 2.0 * n * a.shape[1] * b.shape[1] / best / 1e12
+
+
+def peak_probes(dev) -> dict:
+    """Dense GEMM rates measured on this GPU through cuBLAS (torch.matmul), each timed alone,
+    best of 5 after warm-up: TF32 (float32 operands with TF32 tensor math, 8192^3) and FP64
+    (4096^3). They are the denominators of the TF32 and FP64 rooflines."""
+    import torch
+    out = {}
+    prev = torch.backends.cuda.matmul.allow_tf32
+    try:
+        torch.backends.cuda.matmul.allow_tf32 = True
+        a = torch.randn(8192, 8192, device=dev)
+        b = torch.randn(8192, 8192, device=dev)
+        out["tf32_tflops"] = _gemm_tflops(torch, a, b)
+        del a, b
+        a = torch.randn(4096, 4096, device=dev, dtype=torch.float64)
+        b = torch.randn(4096, 4096, device=dev, dtype=torch.float64)
+        out["fp64_tflops"] = _gemm_tflops(torch, a, b)
+        del a, b
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+        torch.cuda.empty_cache()
+    out["how"] = ("torch.matmul burst, best of 5 (CUDA events): float32 8192^3 with TF32 "
+                  "tensor math; float64 4096^3")
+    return out
+
+
+# ------------------------------------------------------------------------------------------
+# accuracy of a result against FP64 (computed here with torch in float64 on the GPU)
+# ------------------------------------------------------------------------------------------
+def accuracy(L, G, X, X2, alpha, beta, D, I, mode_name, nsample=256, seed=17):
+    """On `nsample` seeded rows: the FP64 distances of the returned ids (float inputs upcast,
+    the caller's norms, (-2<q,c> + |c|^2) + |q|^2 clamped at 0) against the returned values
+    (max relative error), and whether they equal the k smallest FP64 distances of the row over
+    all candidates (exact recall, tie-robust). For tensor-core modes also max |d' - d| / E of
+    the approximate distances of `nsample` rows against all candidates."""
+    import ctypes
+    import torch
+    from rnn_b200 import workloads as W
+    n, k = D.shape
+    rows = torch.from_numpy(np.sort(W.permutation(seed, n)[:nsample]).astype(np.int64)).to(
+        D.device)
+    q = beta[rows].long()
+    Xq = X[q].double()
+    qq = X2[q].double()
+    Xc = X[alpha.long()].double()
+    cc = X2[alpha.long()].double()
+    full = torch.clamp(-2.0 * Xq @ Xc.T + cc[None, :] + qq[:, None], min=0.0)
+    best = torch.topk(full, k, dim=1, largest=False, sorted=True).values
+    ids = I[rows].long()
+    ok = ids >= 0
+    # FP64 distance of each returned id, read from the same block (position of the id in the
+    # candidate list; a repeated id has one distance)
+    pos = torch.full((X.shape[0],), -1, dtype=torch.long, device=D.device)
+    pos[alpha.long()] = torch.arange(alpha.numel(), device=D.device)
+    pid = pos[ids.clamp(min=0)]
+    ok = ok & (pid >= 0)
+    got = torch.where(ok, full.gather(1, pid.clamp(min=0)), torch.full_like(best, float("inf")))
+    rel = ((D[rows].double() - got).abs() / got.clamp(min=1e-30))[ok]
+    exact_rows = int((torch.sort(got, dim=1).values == best).all(dim=1).sum().item())
+    res = {"rows_checked": int(nsample), "rows_exact_fp64_recall": exact_rows,
+           "max_rel_dist_err": float(rel.max().item()) if rel.numel() else 0.0}
+    del full
+    tc = {"tf32": 2, "bf16": 3, "bf16x3": 4}.get(mode_name)
+    if tc is not None:
+        f = L.gsknn_tc_distances
+        vp, ci, ll = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong
+        f.argtypes = [ci, ci, ci, ci, ci, vp, vp, ll, vp, vp, vp, ll, vp, vp, vp, ci, vp, ll,
+                      vp, vp]
+        f.restype = ci
+        m, d = alpha.numel(), X.shape[1]
+        sub = beta[rows].contiguous()
+        Dd = torch.full((nsample, k), float("inf"), device=D.device)
+        Id = torch.full((nsample, k), -1, dtype=torch.int32, device=D.device)
+        C = torch.empty((nsample, m), device=D.device)
+        margin = torch.zeros(nsample, device=D.device)
+        st = torch.cuda.current_stream(D.device)
+        rc = f(tc, m, nsample, d, k, X.data_ptr(), X2.data_ptr(), X.shape[0], alpha.data_ptr(),
+               X.data_ptr(), X2.data_ptr(), X.shape[0], sub.data_ptr(), Dd.data_ptr(),
+               Id.data_ptr(), k, C.data_ptr(), m, margin.data_ptr(), st.cuda_stream)
+        torch.cuda.synchronize()
+        if rc == 0:
+            exu = -2.0 * Xq @ Xc.T + cc[None, :] + qq[:, None]
+            E = margin.double()[:, None] / 2.0
+            res["max_err_over_E"] = float(((C.double() - exu).abs() / E).max().item())
+            res["median_E"] = float(E.median().item())
+            del exu
+        del C
+    torch.cuda.empty_cache()
+    return res
+
+
+# ------------------------------------------------------------------------------------------
+# config 1: plain dgsknn, FP64
+# ------------------------------------------------------------------------------------------
+def fp64_config1(L, G, W, dev, peaks, args):
+    """dgsknn in float64: N=8192, d=32, U[0,1), 4096 queries, 4096 candidates, k=16; one step =
+    two calls, the second with a fresh candidate list merging into the same heaps."""
+    import ctypes
+    import torch
+    p, alpha2 = W.config1(1)
+    X = torch.from_numpy(p.X).to(dev)
+    X2 = torch.from_numpy(p.X2).to(dev)
+    a1 = torch.from_numpy(p.alpha).to(dev)
+    a2 = torch.from_numpy(alpha2).to(dev)
+    b = torch.from_numpy(p.beta).to(dev)
+    D = torch.empty((p.n, p.k), dtype=torch.float64, device=dev)
+    I = torch.empty((p.n, p.k), dtype=torch.int32, device=dev)
+    st = torch.cuda.current_stream(dev)
+    N = p.X.shape[0]
+
+    def step():
+        D.fill_(float("inf"))
+        I.fill_(-1)
+        for a in (a1, a2):
+            rc = L.gsknn_d_device(p.m, p.n, p.d, p.k, X.data_ptr(), X2.data_ptr(), N,
+                                  a.data_ptr(), X.data_ptr(), X2.data_ptr(), N, b.data_ptr(),
+                                  D.data_ptr(), I.data_ptr(), p.k, st.cuda_stream)
+            if rc != 0:
+                raise RuntimeError(G.last_error())
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    steps = max(20, args.steps)
+    read_trace(L)
+    L.gsknn_trace_enable(1)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(steps):
+        step()
+    e1.record(st)
+    torch.cuda.synchronize()
+    L.gsknn_trace_enable(0)
+    tr = read_trace(L)
+    ms = e0.elapsed_time(e1) / steps
+    evals = 2.0 * p.n * p.m
+    if L.gsknn_stream_status(ctypes.c_void_p(st.cuda_stream)) != 0:
+        raise RuntimeError(G.last_error())
+    # accuracy: both calls' merged result against FP64 over the union of the candidate lists
+    acc = accuracy(L, G, X, X2, torch.cat([a1, a2]), b, D, I, "fp64", nsample=512)
+    kern = tr.get("fused_knn_simt")
+    roof = None
+    if kern and peaks.get("fp64_tflops"):
+        kms = kern["ms"] / kern["launches"]
+        ach = p.n * p.m * (2 * p.d + 3) / (kms * 1e-3) / 1e12
+        roof = {"bound": "fp64", "achieved": ach, "peak": peaks["fp64_tflops"],
+                "unit": "TFLOP/s", "frac": ach / peaks["fp64_tflops"], "kernel": "fused_knn_simt",
+                "kernel_ms": kms, "peak_source": "measured FP64 DGEMM rate (peak_probes)"}
+    # e2e: dgsknn through heap_t with host buffers, both calls per step
+    h = G.Heap(p.n, p.k, 1.79e308, double=True)
+
+    def host_step():
+        h.D[:] = 1.79e308
+        h.I[:] = -1
+        G.gsknn_heap(p.k, p.X, p.X2, p.alpha, p.X, p.X2, p.beta, h)
+        G.gsknn_heap(p.k, p.X, p.X2, alpha2, p.X, p.X2, p.beta, h)
+
+    for _ in range(3):
+        host_step()
+    hs = max(10, args.steps)
+    t0 = time.perf_counter()
+    for _ in range(hs):
+        host_step()
+    th = (time.perf_counter() - t0) / hs
+    h.free()
+    # per call: the table's referenced row range with norms, both index lists, heaps both ways
+    h2d = 2 * (N * (p.d + 1) * 8 + (p.n + p.m) * 4 + p.n * p.k * 12)
+    d2h = 2 * p.n * p.k * 12
+    res = {"workload": "plain dgsknn float64: N=8192 d=32 U[0,1), 4096 queries x 4096 "
+                       "candidates, k=16, two merging calls per step",
+           "value": evals / (ms * 1e-3), "unit": "distance-evals/s", "ms_per_step": ms,
+           "kernels": tr, "roofline": roof, "accuracy": acc,
+           "e2e": {"value": evals / th, "unit": "distance-evals/s", "ms_per_step": th * 1e3,
+                   "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                   "api": "dgsknn (heap_t from heapCreate_d, host buffers)"}}
+    if not args.no_cpu_baseline:
+        try:
+            res["cpu_baseline"] = config1_cpu_baseline(min(args.cpu_seconds, 10.0),
+                                                      args.threads)
+        except Exception as e:  # reported, not fatal
+            res["cpu_baseline"] = {"error": str(e)[-400:]}
+    return res
 
 def run_ours(args, rank, world, local_rank):
     import torch
@@ -426,6 +684,10 @@ def run_ours(args, rank, world, local_rank):
     barrier = RP.barrier
 
     out = {}
+    if not args.profile_only and world == 1:
+        probes = peak_probes(dev)
+        peaks["tf32_tflops"] = probes["tf32_tflops"]
+        peaks["fp64_tflops"] = probes["fp64_tflops"]
     if args.batch_only:
         return batching_form(L, G, W, dev, peaks, args, args.threads)
     if args.serve_only:
@@ -463,16 +725,19 @@ def run_ours(args, rank, world, local_rank):
         }
         if args.profile_only:
             return out
+        out["accuracy"] = accuracy(L, G, prob.X, prob.X2, prob.alpha, prob.beta, prob.D,
+                                   prob.I, used)
         out["e2e"] = e2e_host(L, G, p, beta_h, args)
         if world == 1:
             modes = {}
             for nm in ("fp32", "tf32", "bf16", "bf16x3"):
-                # plain BF16 at d = 64 overflows the band logs on this data and goes through
-                # the exact brute-force fallback (seconds per call): one step is enough
+                # plain BF16 at d = 64 overflows the band logs on this data; one step is enough
                 steps = 2 if nm == "fp32" else 1 if nm == "bf16" else 5
                 mms, tr = timed(L, G, prob, name2mode[nm], steps, 1)
                 modes[nm] = {"ms_per_step": mms, "value": prob.evals / (mms * 1e-3),
-                             "roofline": roofline(nm, prob, tr, peaks, clk)}
+                             "roofline": roofline(nm, prob, tr, peaks, clk),
+                             "accuracy": accuracy(L, G, prob.X, prob.X2, prob.alpha,
+                                                  prob.beta, prob.D, prob.I, nm)}
             out["modes"] = modes
         del prob
         torch.cuda.empty_cache()
@@ -481,6 +746,8 @@ def run_ours(args, rank, world, local_rank):
         if args.precision_only:
             return pf
         out["precision_form"] = pf
+        if not args.profile_only:
+            out["fp64_config1"] = fp64_config1(L, G, W, dev, peaks, args)
         if not args.no_batch and not args.profile_only:
             out["batching_form"] = batching_form(L, G, W, dev, peaks, args, args.threads)
         if not args.no_serve and not args.profile_only:
@@ -516,6 +783,9 @@ def precision_form(L, G, W, dev, peaks, args):
         ms, tr = timed(L, G, prob, name2mode[nm], steps, 0 if args.profile_only else 1)
         res[nm] = {"ms_per_step": ms, "value": prob.evals / (ms * 1e-3),
                    "roofline": roofline(nm, prob, tr, peaks, None), "kernels": tr}
+        if not args.profile_only:
+            res[nm]["accuracy"] = accuracy(L, G, prob.X, prob.X2, prob.alpha, prob.beta,
+                                           prob.D, prob.I, nm)
     if "fp32" in res:
         base = res["fp32"]["value"]
         for nm in ("tf32", "bf16", "bf16x3"):
@@ -803,6 +1073,64 @@ def e2e_host(L, G, p, beta_h, args):
             "api": "sgsknn_var1 (host pointers, pageable numpy buffers), default mode"}
 
 
+
+def summarize(out: dict) -> dict:
+    """Compact figures of every leg, placed last in the JSON line so that a reader keeping only
+    the tail of the line still has them."""
+    def r(x, n=4):
+        return None if x is None else float(f"{x:.{n}g}")
+    sm = {}
+    if "value" in out:
+        sm["headline"] = {"evals_per_s": r(out["value"]), "ms": r(out.get("ms_per_step")),
+                          "e2e_evals_per_s": r((out.get("e2e") or {}).get("value")),
+                          "roofline_frac": r((out.get("roofline") or {}).get("frac")),
+                          "mode": out.get("mode"),
+                          "rows_exact": (out.get("accuracy") or {}).get("rows_exact_fp64_recall"),
+                          "max_rel_dist_err": r((out.get("accuracy") or {}).get(
+                              "max_rel_dist_err"), 3)}
+    if "modes" in out:
+        base = out["modes"]["fp32"]["value"]
+        sm["modes"] = {nm: {"ms": r(v["ms_per_step"]),
+                            "x_vs_fp32": r(v["value"] / base, 3),
+                            "frac": r((v.get("roofline") or {}).get("frac"), 3),
+                            "err_over_E": r((v.get("accuracy") or {}).get("max_err_over_E"), 3),
+                            "rows_exact": (v.get("accuracy") or {}).get(
+                                "rows_exact_fp64_recall")}
+                       for nm, v in out["modes"].items()}
+    pf = out.get("precision_form")
+    if pf:
+        sm["precision_form"] = {nm: {"ms": r(pf[nm]["ms_per_step"]),
+                                     "x_vs_fp32": r(pf[nm].get("speedup_vs_plain_fp32"), 3),
+                                     "frac": r((pf[nm].get("roofline") or {}).get("frac"), 3),
+                                     "err_over_E": r((pf[nm].get("accuracy") or {}).get(
+                                         "max_err_over_E"), 3),
+                                     "max_rel_dist_err": r((pf[nm].get("accuracy") or {}).get(
+                                         "max_rel_dist_err"), 3),
+                                     "rows_exact": (pf[nm].get("accuracy") or {}).get(
+                                         "rows_exact_fp64_recall")}
+                                for nm in ("fp32", "tf32", "bf16", "bf16x3") if nm in pf}
+    c1 = out.get("fp64_config1")
+    if c1:
+        sm["fp64_config1"] = {"evals_per_s": r(c1["value"]), "ms": r(c1["ms_per_step"]),
+                              "e2e_evals_per_s": r(c1["e2e"]["value"]),
+                              "cpu_evals_per_s": r((c1.get("cpu_baseline") or {}).get("value")),
+                              "frac": r((c1.get("roofline") or {}).get("frac"), 3),
+                              "rows_exact": c1["accuracy"]["rows_exact_fp64_recall"]}
+    bf = out.get("batching_form")
+    if bf:
+        sm["batching"] = {"evals_per_s": r(bf.get("value")), "ms_per_pass": r(
+            bf.get("ms_per_pass")), "cpu_evals_per_s": r((bf.get("cpu_baseline") or {}).get(
+                "value"))}
+    sv = out.get("serving_form")
+    if sv:
+        lat = sv.get("latency_ms") or {}
+        sm["serving"] = {"p50_ms": r(lat.get("p50")), "p99_ms": r(lat.get("p99")),
+                         "evals_per_s": r(sv.get("value"))}
+    cb = out.get("cpu_baseline")
+    if isinstance(cb, dict) and "value" in cb:
+        sm["cpu_baseline_evals_per_s"] = r(cb["value"])
+    return sm
+
 def main():
     args = parse()
     if args.cpu_worker:
@@ -855,6 +1183,8 @@ def main():
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
+        if world == 1 and not args.profile_only:
+            out["summary"] = summarize(out)
         print(json.dumps(out), flush=True)
 
 

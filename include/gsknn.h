@@ -228,13 +228,20 @@ int gsknn_stream_status(void *stream);
  *   - the packed problem must fit the fixed scratch: about (m + n) * round_up(d, 16) * 4 bytes
  *     of panels plus n * k * 8 bytes of partial lists; larger problems are rejected with
  *     GSKNN_ERR_UNSUPPORTED and a message (nothing is launched), use gsknn_s_device for them;
+ *   - k <= 256 (the fused kernel's list size); larger k is rejected with
+ *     GSKNN_ERR_UNSUPPORTED (gsknn_s_device takes it through its explicit-distance path);
  *   - the first call on a device looks up the array's device address (cudaGetSymbolAddress)
- *     with that device current; make that first call before any stream capture;
+ *     with that device current and keeps it for the life of the process; make that first
+ *     call before any stream capture, and do not use the entry point across a device reset
+ *     (cudaDeviceReset), after which the kept address no longer names the array;
  *   - every call on a device shares the one array and it keeps the last call's contents:
  *     calls whose work may overlap on the GPU (different streams without ordering) race and
  *     corrupt each other's results; serialise them, e.g. on one stream;
  *   - `status` (device pointer, may be NULL) is cleared and then receives GSKNN_ERR_INDEX if
- *     an alpha/beta entry lies outside its table; with NULL the check still guards the reads.
+ *     an alpha/beta entry lies outside its table; with NULL the check still guards the reads
+ *     but the error is not observable. gsknn_stream_status() does not cover this entry point
+ *     (it reports the per-stream word of the caching entry points): pass `status` to see
+ *     index errors.
  * Returns 0 when the work was enqueued on `stream`. */
 int gsknn_s_device_noalloc(int m, int n, int d, int k, const float *XA, const float *XA2,
                            long long nA, const int *alpha, const float *XB, const float *XB2,

@@ -100,10 +100,15 @@ gsknn_table_t *gsknn_table_open(const char *path) {
   TableHeader h{};
   const bool head_ok = ::fstat(fd, &st) == 0 && (size_t)st.st_size >= sizeof(h) &&
                        ::pread(fd, &h, sizeof(h), 0) == (ssize_t)sizeof(h);
-  const bool valid = head_ok && std::memcmp(h.magic, kMagic, 8) == 0 && h.version == 1 &&
-                     h.d > 0 && h.N > 0 && h.rows_off == sizeof(h) &&
+  // sizes are checked before any product is formed, so no header can wrap the arithmetic:
+  // d and N fit an int, and N * (d + 1) * 4 bytes (rows and norms) fits 63 bits
+  const bool sizes_ok = head_ok && h.d > 0 && h.d <= 0x7fffffffULL && h.N > 0 &&
+                        h.N <= 0x7fffffffULL &&
+                        h.N <= ((uint64_t)1 << 62) / (4 * ((uint64_t)h.d + 1));
+  const bool valid = sizes_ok && std::memcmp(h.magic, kMagic, 8) == 0 && h.version == 1 &&
+                     h.rows_off == sizeof(h) &&
                      h.norms_off == h.rows_off + h.N * h.d * 4 &&
-                     (uint64_t)st.st_size >= h.norms_off + h.N * 4 && h.N <= 0x7fffffffULL;
+                     (uint64_t)st.st_size >= h.norms_off + h.N * 4;
   if (!valid) {
     ::close(fd);
     set_status(GSKNN_ERR_ARG, "gsknn_table_open: %s is not a point table of this format", path);

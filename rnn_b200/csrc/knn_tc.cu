@@ -286,20 +286,9 @@ __device__ __noinline__ int log_compact(uint2 *lg, int cnt, float thr) {
 
 constexpr int PEND = 8;  // heap inserts a lane may defer before the warp flushes them
 
-// Log the candidate (when `act`) and, for heap owners, defer its heap insert into a small
-// register ring (filled through compile-time indices so it stays in registers). Branch-free:
-// every lane of the warp runs it, with predicates instead of divergent branches.
-__device__ __forceinline__ void epi_candidate(EpiState &s, float v, uint32_t id, bool act,
-                                              uint2 *lg, int logcap, bool owner,
-                                              float (&pend)[PEND], int &np) {
-  const float dp = v + s.qn;
-  const bool take = act && dp <= s.thr;
-  s.n_ev += take ? 1u : 0u;
-  const bool room = s.cnt < logcap;
-  if (take && !s.ovf && room) lg[s.cnt] = make_uint2(__float_as_uint(dp), id);
-  s.cnt += (take && !s.ovf && room) ? 1 : 0;
-  s.ovf |= (take && !room) ? 1 : 0;
-  const bool ins = take && owner && dp < s.root;
+// Defer the heap insert of `dp` (when `ins`) into a small register ring, filled through
+// compile-time indices so it stays in registers.
+__device__ __forceinline__ void epi_defer(float dp, bool ins, float (&pend)[PEND], int &np) {
 #pragma unroll
   for (int j = 0; j < PEND; j++) pend[j] = (ins && j == np) ? dp : pend[j];
   np += ins ? 1 : 0;
@@ -552,10 +541,14 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         if (col < p.dbg_ncols) p.dbg[(size_t)gq * p.dbg_ld + col] = __uint_as_float(r[i]) + s.qn;
       }
     };
-    // Slow part, for a chunk in which some lane has a candidate under its threshold: a
-    // warp-convergent pass in which every lane with pending candidates handles one of them per
-    // iteration (selected from its registers by index).
-    auto slow = [&](const uint32_t (&r)[32], size_t cbase, int c0) {
+    // Slow part, for a chunk in which some lane has a candidate under its threshold. Every
+    // lane logs its own survivors, one predicated compare-and-store per column through
+    // compile-time register indices (no runtime selection, no loop over survivors), and the
+    // row's heap takes the chunk's minimum. The heap therefore holds the k smallest of a subset
+    // of the candidates seen (one real candidate per entry), so its root still bounds the k-th
+    // smallest approximate distance from above, and every candidate within 2E of the final
+    // k-th stays under the threshold and is logged.
+    auto slow = [&](const uint32_t (&r)[32], float mn, size_t cbase, int c0) {
       // a chunk appends at most 32 entries per lane: make room first, all lanes together
       if (__any_sync(FULL_MASK, s.cnt > p.logcap - 32)) {
         if (s.cnt > p.logcap - 32 && !s.ovf) {
@@ -563,39 +556,24 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           if (s.cnt > p.logcap - 32) s.ovf = 1;
         }
       }
-      // pass mask as an OR tree (depth 5), built by every lane: on this path some lane always
-      // needs it, so a guard would only add a divergent branch
-      uint32_t m16[16];
-#pragma unroll
-      for (int j = 0; j < 16; j++)
-        m16[j] = (__uint_as_float(r[2 * j]) <= s.Tv ? 1u << (2 * j) : 0u) |
-                 (__uint_as_float(r[2 * j + 1]) <= s.Tv ? 1u << (2 * j + 1) : 0u);
-#pragma unroll
-      for (int w = 8; w >= 1; w >>= 1)
-#pragma unroll
-        for (int j = 0; j < w; j++) m16[j] = m16[2 * j] | m16[2 * j + 1];
-      uint32_t mask = m16[0];
       s.n_sc++;
-      while (__any_sync(FULL_MASK, mask != 0)) {
-        s.n_it++;
-        // every lane steps: its lowest pending column, or none (act false)
-        const bool act = mask != 0;
-        const int i = (__ffs(mask) - 1) & 31;
-        mask &= mask - 1;
-        // v[i] for a runtime i: a 5-level select tree on the bits of i
-        float t16[16];
+      const float Tv = s.ovf ? -Num<float>::inf() : s.Tv;
+      const uint32_t pos = (uint32_t)(cbase + c0);
+      int cnt = s.cnt;
 #pragma unroll
-        for (int j = 0; j < 16; j++) t16[j] = __uint_as_float((i & 16) ? r[j + 16] : r[j]);
-#pragma unroll
-        for (int w = 8, bit = 8; w >= 1; w >>= 1, bit >>= 1)
-#pragma unroll
-          for (int j = 0; j < w; j++) t16[j] = (i & bit) ? t16[j + w] : t16[j];
-        // the log keeps the packed candidate position; the re-rank maps it to the id
-        epi_candidate(s, t16[0], (uint32_t)(cbase + c0 + i), act, lg, p.logcap, owner, pend,
-                      np);
-        if (__any_sync(FULL_MASK, np == PEND)) {
-          if (owner) epi_flush(s, heap, row, p.k, pend, np, ksh);
+      for (int j = 0; j < 32; j++) {
+        const float v = __uint_as_float(r[j]);
+        if (v <= Tv) {
+          lg[cnt] = make_uint2(__float_as_uint(v + s.qn), pos + (uint32_t)j);
+          cnt++;
         }
+      }
+      s.n_ev += (unsigned)(cnt - s.cnt);
+      s.cnt = cnt;
+      if (owner) {
+        const float dm = mn + s.qn;  // NaN when every column is padding: never inserted
+        epi_defer(dm, dm < s.root, pend, np);
+        if (__any_sync(FULL_MASK, np == PEND)) epi_flush(s, heap, row, p.k, pend, np, ksh);
       }
     };
     // what the query's other splits have found (all bits set = nothing yet); the load for the
@@ -658,8 +636,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             dbg_write(ra, cbase, c0);
             dbg_write(rb, cbase, c0 + 32);
           }
-          if (__any_sync(FULL_MASK, ma <= s.Tv)) slow(ra, cbase, c0);
-          if (__any_sync(FULL_MASK, mb <= s.Tv)) slow(rb, cbase, c0 + 32);
+          if (__any_sync(FULL_MASK, ma <= s.Tv)) slow(ra, ma, cbase, c0);
+          if (__any_sync(FULL_MASK, mb <= s.Tv)) slow(rb, mb, cbase, c0 + 32);
         } else {
           uint32_t ra[32];
           __syncwarp();
@@ -673,7 +651,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           }
           const float ma = fast(ra, cnt, c0);
           if (p.dbg && valid) dbg_write(ra, cbase, c0);
-          if (__any_sync(FULL_MASK, ma <= s.Tv)) slow(ra, cbase, c0);
+          if (__any_sync(FULL_MASK, ma <= s.Tv)) slow(ra, ma, cbase, c0);
         }
       }
     }

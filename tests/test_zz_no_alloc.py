@@ -123,3 +123,32 @@ def test_noalloc_rejects_problems_beyond_its_scratch():
     assert "fixed scratch" in G.last_error()[1]
     torch.cuda.synchronize()
     assert torch.all(I == -1)
+
+
+def test_noalloc_reports_out_of_range_index_and_rejects_large_k():
+    """An alpha/beta entry outside its table reaches the caller's status word (and is never
+    read); k beyond the fused kernel's list size is refused before any launch."""
+    import torch
+    L, f = _bind()
+    dev = torch.device("cuda:0")
+    st = torch.cuda.current_stream(dev)
+    N, d = 500, 16
+    X = torch.rand((N, d), device=dev)
+    X2 = (X.double() ** 2).sum(1).float()
+    alpha = torch.arange(300, dtype=torch.int32, device=dev)
+    beta = torch.arange(300, 340, dtype=torch.int32, device=dev)
+    beta[5] = N  # one past the end of the table
+    D = torch.full((40, 8), float("inf"), device=dev)
+    I = torch.full((40, 8), -1, dtype=torch.int32, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    rc = _call_noalloc(f, X, X2, alpha, beta, D, I, status, st)
+    assert rc == 0, G.last_error()
+    torch.cuda.synchronize()
+    assert int(status.item()) == 4  # GSKNN_ERR_INDEX
+    beta[5] = 5
+    D300 = torch.full((40, 300), float("inf"), device=dev)
+    I300 = torch.full((40, 300), -1, dtype=torch.int32, device=dev)
+    rc = _call_noalloc(f, X, X2, alpha, beta, D300, I300, status, st)
+    assert rc == 5  # GSKNN_ERR_UNSUPPORTED
+    torch.cuda.synchronize()
+    assert torch.all(I300 == -1) and torch.all(torch.isinf(D300))
