@@ -119,6 +119,13 @@ struct TcPlan {
   size_t o_pa, o_pa_lo, o_qn, o_qnrm, o_log, o_logcnt, o_kth, o_kth_shared, o_margin, o_fbl,
       o_fbc;
   size_t cand_bytes;  // prepared-candidate area at the start of the workspace (0: separate)
+  // Escalation: queries whose band log overflowed in this format run again in a narrower one
+  // (esc_mode, 0 = none: they go straight to the FP64 brute force). Its query-side workspace
+  // starts at o_esc; o_ecand holds its candidate panels when the prepared candidates carry
+  // none (packed only when some query overflowed).
+  int esc_mode;
+  size_t o_esc, o_ecand, esc_bytes, ecand_bytes;
+  int sms, max_splits;  // the plan's arguments, to re-derive the escalation pass's plan
   size_t bytes;       // whole workspace
 };
 
@@ -138,10 +145,22 @@ struct TcCand {
   const float *Xc, *Xc2;
   long long nrows_c;
   const int *cidx;
+  // optional panels of the same candidates in a second format (escalation pass; shift, norms,
+  // bounds and ids are shared with the first): efmt is a format of tc_format_of_mode, -1 when
+  // absent
+  int efmt;
+  void *epb, *epb_lo;
 };
 
 int tc_format_of_mode(int mode);
+// The narrower format a tensor-core mode escalates overflowed queries to (0: none).
+int tc_escalation_mode(int nq, int nc, int d, int k, int mode, int sms);
 size_t tc_cand_bytes(int nc, int d, int mode);
+// Bytes of candidate panels in `mode`'s format alone (the escalation panels of a prepared set).
+size_t tc_cand_panel_bytes(int nc, int d, int mode);
+// Packs the escalation panels of prepared candidates C in `mode`'s format into `mem`.
+cudaError_t tc_cand_prepare_escalation(TcCand *C, void *mem, int mode, int *status,
+                                       cudaStream_t st);
 cudaError_t tc_cand_prepare(TcCand *C, void *mem, int nc, int d, int mode, const float *Xc,
                             const float *Xc2, long long nrows_c, const int *cidx, int *status,
                             cudaStream_t st);

@@ -198,6 +198,7 @@ struct Engine {
   size_t heap_budget;
   TcCand C{};
   void *cand_mem = nullptr;
+  void *ecand_mem = nullptr;  // the resident set's panels in the escalation format
   int *cidx = nullptr, *status = nullptr;
   char *arena_mem = nullptr;
   std::unique_ptr<serve::Arena> arena;
@@ -502,7 +503,12 @@ gsknn_serve_t *gsknn_serve_create(const float *R, const float *R2, int nref, int
       E->ws_bytes = std::max(E->ws_bytes, P.bytes);
     }
   const size_t cb = tc_cand_bytes(nref, d, mode);
-  bool ok = cudaMalloc(&E->cand_mem, cb) == cudaSuccess &&
+  // queries whose band log overflows in this format run again in a narrower one: its panels of
+  // the resident set are prepared once, beside the first
+  const int esc = tc_escalation_mode(E->max_q, nref, d, max_k, mode, E->sms);
+  bool ok = (!esc || cudaMalloc(&E->ecand_mem, tc_cand_panel_bytes(nref, d, esc)) ==
+                         cudaSuccess) &&
+            cudaMalloc(&E->cand_mem, cb) == cudaSuccess &&
             cudaMalloc((void **)&E->cidx, (size_t)nref * 4) == cudaSuccess &&
             cudaMalloc((void **)&E->status, 4) == cudaSuccess &&
             cudaMalloc((void **)&E->arena_mem, heap_budget) == cudaSuccess;
@@ -519,6 +525,8 @@ gsknn_serve_t *gsknn_serve_create(const float *R, const float *R2, int nref, int
   cudaMemsetAsync(E->status, 0, 4, st0);
   cudaError_t e = tc_cand_prepare(&E->C, E->cand_mem, nref, d, mode, R, R2, nref, E->cidx,
                                   E->status, st0);
+  if (e == cudaSuccess && esc)
+    e = tc_cand_prepare_escalation(&E->C, E->ecand_mem, esc, E->status, st0);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st0);
   int st = 0;
   if (e == cudaSuccess) e = cudaMemcpy(&st, E->status, 4, cudaMemcpyDeviceToHost);
@@ -735,6 +743,7 @@ void gsknn_serve_destroy(gsknn_serve_t *eng) {
     if (s.st) cudaStreamDestroy(s.st);
   }
   cudaFree(E->cand_mem);
+  cudaFree(E->ecand_mem);
   cudaFree(E->cidx);
   cudaFree(E->status);
   cudaFree(E->arena_mem);

@@ -108,18 +108,29 @@ __device__ __forceinline__ uint32_t to_tf32(float x) {
 }
 
 // fmt: 0 = TF32 (4-byte panel), 1 = BF16, 2 = split BF16 (hi and lo panels)
+// Optional forms: `dcount` (device) replaces `count` and limits the panel to the tiles it needs;
+// `rowmap` packs point idx[rowmap[r]] as row r; `gate` (device) skips all work when it reads 0;
+// a null `enorm` writes the panels only (norms, bounds, ids and statistics are left alone).
 __global__ void __launch_bounds__(256) tc_pack(
     int fmt, const float *__restrict__ X, const float *__restrict__ X2, int d, int d_pad,
     long long nrows, const int *__restrict__ idx, int count, int rows_pad,
     const float *__restrict__ mu, const double *__restrict__ mu2, int is_cand, void *panel,
     void *panel_lo, float *__restrict__ enorm, float *__restrict__ cnrm,
-    uint32_t *__restrict__ ids, unsigned *__restrict__ stats, int *__restrict__ status) {
+    uint32_t *__restrict__ ids, unsigned *__restrict__ stats, int *__restrict__ status,
+    const int *__restrict__ dcount = nullptr, const int *__restrict__ rowmap = nullptr,
+    const int *__restrict__ gate = nullptr) {
   const int lane = threadIdx.x & 31;
   const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (gate && *gate == 0) return;
+  if (dcount) {
+    count = *dcount;
+    const int used = ((count + TC_M - 1) / TC_M) * TC_M;
+    if (used < rows_pad) rows_pad = used;
+  }
   if (r >= rows_pad) return;
   long long row = -1;
   if (r < count) {
-    row = idx[r];
+    row = idx[rowmap ? rowmap[r] : r];
     if (row < 0 || row >= nrows) {
       if (lane == 0) atomicExch(status, GSKNN_ERR_INDEX);
       row = -1;
@@ -151,7 +162,7 @@ __global__ void __launch_bounds__(256) tc_pack(
     s2 += __shfl_xor_sync(FULL_MASK, s2, o);
     smx += __shfl_xor_sync(FULL_MASK, smx, o);
   }
-  if (lane == 0) {
+  if (lane == 0 && enorm) {
     if (row >= 0) {
       // |x - mu|^2 expressed through the caller's norm: X2 - 2 mu.x + mu.mu
       const double en = (double)X2[row] - 2.0 * smx + *mu2;
@@ -198,6 +209,10 @@ struct TcParams {
   long long dbg_ld;
   long long dbg_ncols;
   unsigned long long *counters;  // optional diagnostics (5 counters), may be null
+  // optional (escalation pass): the query count on the device (Q is then the capacity and the
+  // stride of the per-query arrays) and the heap row of each query
+  const int *dQ;
+  const int *rowmap;
 };
 
 struct SmemLayout {
@@ -241,7 +256,9 @@ struct EpiState {
 __device__ __forceinline__ void refresh_threshold(EpiState &s) {
   float t = fminf(s.root, s.shared) + s.E2;
   s.thr = t < s.thr0 ? t : s.thr0;
-  if (s.thr == -Num<float>::inf()) {  // padding rows past the last query: never admit
+  // padding rows past the last query never admit; nor does a row whose log overflowed (the
+  // query is finished by a later pass), so its chunks stop taking the slow path
+  if (s.thr == -Num<float>::inf() || s.ovf) {
     s.Tv = -Num<float>::inf();
     return;
   }
@@ -320,6 +337,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
            const __grid_constant__ CUtensorMap tB, const __grid_constant__ CUtensorMap tBlo,
            const TcParams p) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // escalation pass: launched for the largest possible query count, the tiles past the count
+  // on the device exit before any set-up
+  const int Qn = p.dQ ? *p.dQ : p.Q;
+  if ((int)blockIdx.x * TC_M >= Qn) return;
   const uint32_t raw = su32(smem_raw);
   unsigned char *smem = smem_raw + ((1024u - (raw & 1023u)) & 1023u);
   const SmemLayout L = tc_smem_layout(p.nkc, p.a_terms, p.b_terms, p.N, p.NST, p.k);
@@ -464,7 +485,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     const bool owner = part == 0;
     const int row = lq * 32 + lane;
     const int gq = qt * TC_M + row;
-    const bool valid = gq < p.Q;
+    const bool valid = gq < Qn;
     EpiState s;
     s.cnt = 0;
     s.ovf = 0;
@@ -488,7 +509,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       s.E2 = 2.0f * E;
       if (p.Din) {
         float mx = -Num<float>::inf();
-        const float *rowD = p.Din + (size_t)gq * p.ldD;
+        const float *rowD = p.Din + (size_t)(p.rowmap ? p.rowmap[gq] : gq) * p.ldD;
         for (int j = 0; j < p.k; j++) mx = fmaxf(mx, rowD[j]);
         if (mx > -Num<float>::inf()) s.thr0 = mx + s.E2;
       }
@@ -553,7 +574,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       if (__any_sync(FULL_MASK, s.cnt > p.logcap - 32)) {
         if (s.cnt > p.logcap - 32 && !s.ovf) {
           s.cnt = log_compact(lg, s.cnt, s.thr);
-          if (s.cnt > p.logcap - 32) s.ovf = 1;
+          if (s.cnt > p.logcap - 32) {
+            s.ovf = 1;
+            refresh_threshold(s);
+          }
         }
       }
       s.n_sc++;
@@ -698,6 +722,8 @@ struct RerankParams {
   int *fallback_list;
   int *fallback_count;
   unsigned long long *counters;  // optional: [5] entries scanned, [6] exact distances
+  const int *dQ;      // optional: query count on the device (Q is then the stride)
+  const int *rowmap;  // optional: heap row (and query position in qidx) of each query
 };
 
 // Exact squared distance of the oracle: (-2 <q,c> + |c|^2) + |q|^2 in FP64 from float inputs,
@@ -770,8 +796,9 @@ __global__ void __launch_bounds__(256) tc_rerank(RerankParams p) {
   __shared__ uint32_t rr_stage[8][64];
   const int lane = threadIdx.x & 31;
   const int q = blockIdx.x * 8 + (threadIdx.x >> 5);
-  if (q >= p.Q) return;
-  // overflowed logs: the whole query goes to the brute-force pass
+  if (q >= (p.dQ ? *p.dQ : p.Q)) return;
+  const int hr = p.rowmap ? p.rowmap[q] : q;  // heap row and query position
+  // overflowed logs: the query goes to the next pass (a narrower format, or brute force)
   bool ovf = false;
   float T = __uint_as_float(p.kth_shared[q]);  // NaN (all bits set) when nothing was published
   for (int s = 0; s < p.S; s++) {
@@ -779,7 +806,7 @@ __global__ void __launch_bounds__(256) tc_rerank(RerankParams p) {
     T = fminf(T, p.kth[(size_t)s * p.Q + q]);
   }
   if (ovf) {
-    if (lane == 0) p.fallback_list[atomicAdd(p.fallback_count, 1)] = q;
+    if (lane == 0) p.fallback_list[atomicAdd(p.fallback_count, 1)] = hr;
     return;
   }
   const float E2 = p.margin[q];
@@ -817,14 +844,14 @@ __global__ void __launch_bounds__(256) tc_rerank(RerankParams p) {
   float thr = T + E2;
   {
     float mx = -Num<float>::inf();
-    for (int j = lane; j < p.k; j += 32) mx = fmaxf(mx, p.D[(size_t)q * p.ldD + j]);
+    for (int j = lane; j < p.k; j += 32) mx = fmaxf(mx, p.D[(size_t)hr * p.ldD + j]);
     for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(FULL_MASK, mx, o));
     if (mx > -Num<float>::inf()) thr = fminf(thr, mx + E2);
   }
   double ld[E];
   uint32_t li[E];
-  load_heap_row<E>(p.D, p.I, p.ldD, q, p.k, ld, li, lane);
-  const long long qrow = p.qidx[q];
+  load_heap_row<E>(p.D, p.I, p.ldD, hr, p.k, ld, li, lane);
+  const long long qrow = p.qidx[hr];
   const float *qv = p.Xq + qrow * p.d;
   const double qq = (double)p.Xq2[qrow];
   // Pass 2: band entries are compacted into a per-warp staging list; every 32 of them each lane
@@ -873,7 +900,7 @@ __global__ void __launch_bounds__(256) tc_rerank(RerankParams p) {
     }
   }
   if (nb > 0) flush(nb);
-  write_heap_row<E>(p.D, p.I, p.ldD, q, p.k, ld, li, lane);
+  write_heap_row<E>(p.D, p.I, p.ldD, hr, p.k, ld, li, lane);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1053,6 +1080,7 @@ cudaError_t tc_cand_prepare(TcCand *C, void *mem, int nc, int d, int mode, const
   C->cnrm = reinterpret_cast<float *>(base + L.o_cnrm);
   C->cid = reinterpret_cast<uint32_t *>(base + L.o_cid);
   C->Xc = Xc; C->Xc2 = Xc2; C->nrows_c = nrows_c; C->cidx = cidx;
+  C->efmt = -1; C->epb = nullptr; C->epb_lo = nullptr;
   cudaError_t e = cudaMemsetAsync(C->stats, 0, 16, st);
   if (e != cudaSuccess) return e;
   const int nsample = std::min(nc, 4096);
@@ -1064,11 +1092,13 @@ cudaError_t tc_cand_prepare(TcCand *C, void *mem, int nc, int d, int mode, const
   return cudaGetLastError();
 }
 
-TcPlan tc_plan(int nq, int nc, int d, int k, int mode, int sms, bool with_cand,
-               int max_splits) {
+static TcPlan tc_plan_base(int nq, int nc, int d, int k, int mode, int sms, bool with_cand,
+                          int max_splits) {
   using namespace tc;
   TcPlan P{};
   P.ok = false;
+  P.sms = sms;
+  P.max_splits = max_splits;
   P.fmt = tc_format_of_mode(mode);
   const int elem = P.fmt == 0 ? 4 : 2;
   const int celems = CHUNK_BYTES / elem;
@@ -1147,6 +1177,47 @@ TcPlan tc_plan(int nq, int nc, int d, int k, int mode, int sms, bool with_cand,
   return P;
 }
 
+static size_t panel_bytes(int r_pad, int d_pad, int fmt) {
+  const size_t one = al256((size_t)r_pad * d_pad * (fmt == 0 ? 4 : 2));
+  return fmt == 2 ? 2 * one : one;
+}
+
+size_t tc_cand_panel_bytes(int nc, int d, int mode) {
+  const CandLayout L = cand_layout(nc, d, mode);
+  return panel_bytes(L.r_pad, L.d_pad, L.fmt);
+}
+
+// Split BF16 has the narrowest band; a query whose BF16 or TF32 log overflowed runs again in it
+// (or, from BF16, in TF32 where the split tiles do not fit).
+int tc_escalation_mode(int nq, int nc, int d, int k, int mode, int sms) {
+  const int fmt = tc_format_of_mode(mode);
+  if (fmt == 2) return 0;
+  if (tc_plan_base(nq, nc, d, k, GSKNN_TC_BF16X3, sms, false, 0).ok) return GSKNN_TC_BF16X3;
+  if (fmt == 1 && tc_plan_base(nq, nc, d, k, GSKNN_TC_TF32, sms, false, 0).ok)
+    return GSKNN_TC_TF32;
+  return 0;
+}
+
+TcPlan tc_plan(int nq, int nc, int d, int k, int mode, int sms, bool with_cand,
+               int max_splits) {
+  TcPlan P = tc_plan_base(nq, nc, d, k, mode, sms, with_cand, max_splits);
+  if (!P.ok) return P;
+  P.esc_mode = tc_escalation_mode(nq, nc, d, k, mode, sms);
+  if (P.esc_mode) {
+    const TcPlan EP = tc_plan_base(nq, nc, d, k, P.esc_mode, sms, false, max_splits);
+    P.o_esc = al256(P.bytes);
+    P.esc_bytes = EP.bytes;
+    size_t off = al256(P.o_esc + EP.bytes);
+    if (with_cand) {  // per-call candidates: their escalation panels live in the workspace
+      P.o_ecand = off;
+      P.ecand_bytes = panel_bytes(EP.r_pad, EP.d_pad, EP.fmt);
+      off = al256(off + P.ecand_bytes);
+    }
+    P.bytes = off;
+  }
+  return P;
+}
+
 cudaError_t tc_run(const TcPlan &P, int nq, int nc, int d, int k, const float *Xq,
                    const float *Xq2, long long nrows_q, const int *qidx, const float *Xc,
                    const float *Xc2, long long nrows_c, const int *cidx, float *D, int *I,
@@ -1165,45 +1236,49 @@ cudaError_t tc_run(const TcPlan &P, int nq, int nc, int d, int k, const float *X
                          dbg_ld, counters, st, hook, hook_ctx);
 }
 
-cudaError_t tc_run_prepared(const TcPlan &P, const TcCand &C, int nq, int d, int k,
-                            const float *Xq, const float *Xq2, long long nrows_q,
-                            const int *qidx, float *D, int *I, int ldD, void *ws, int *status,
-                            float *dbg, long long dbg_ld, unsigned long long *counters,
-                            cudaStream_t st, TraceHook hook, void *hook_ctx) {
+// One approximate pass + re-rank: pack the queries (all of them, or on an escalation pass the
+// `dQ` queries listed in `rowmap`), tc_knn in the plan's format, tc_rerank. Queries whose log
+// overflowed are appended (as heap rows) to the plan's fallback list, whose count sits at
+// base + P.o_fbc.
+static cudaError_t tc_pass(const TcPlan &P, const TcCand &C, void *cand_pb, void *cand_pb_lo,
+                           int nq, int d, int k, const float *Xq, const float *Xq2,
+                           long long nrows_q, const int *qidx, const int *dQ, const int *rowmap,
+                           float *D, int *I, int ldD, char *base, int *status, float *dbg,
+                           long long dbg_ld, unsigned long long *counters, cudaStream_t st,
+                           TraceHook hook, void *hook_ctx, bool escalation) {
   using namespace tc;
-  if (C.fmt != P.fmt || C.d_pad != P.d_pad || C.r_pad != P.r_pad) return cudaErrorInvalidValue;
-  char *base = static_cast<char *>(ws);
   void *pa = base + P.o_pa;
   void *pa_lo = P.fmt == 2 ? base + P.o_pa_lo : nullptr;
   float *qn = reinterpret_cast<float *>(base + P.o_qn);
   float *qnrm = reinterpret_cast<float *>(base + P.o_qnrm);
   int *fbc = reinterpret_cast<int *>(base + P.o_fbc);
-  const int nc = C.nc;
   cudaError_t e = cudaMemsetAsync(fbc, 0, 16, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(base + P.o_kth_shared, 0xFF, (size_t)nq * 4, st);
   if (e != cudaSuccess) return e;
-
   // tracer brackets; `nk` = kernels of this file launched inside the bracket
   auto mark = [&](const char *name, bool begin, int nk = 0) {
     if (hook) hook(hook_ctx, name, begin, st, nk);
   };
-  mark("tc_pack", true);
+  const char *n_pack = escalation ? "tc_escalate" : "tc_pack";
+  const char *n_knn = escalation ? "tc_escalate" : "tc_knn";
+  const char *n_rr = escalation ? "tc_escalate" : "tc_rerank";
+  mark(n_pack, true);
   tc_pack<<<(P.q_pad + 7) / 8, 256, 0, st>>>(P.fmt, Xq, Xq2, d, P.d_pad, nrows_q, qidx, nq,
                                             P.q_pad, C.mu, C.mu2, 0, pa, pa_lo, qn, qnrm,
-                                            nullptr, C.stats, status);
+                                            nullptr, C.stats, status, dQ, rowmap, nullptr);
   e = cudaGetLastError();
-  mark("tc_pack", false, 1);  // query pack
+  mark(n_pack, false, 1);  // query pack
   if (e != cudaSuccess) return e;
 
   CUtensorMap mA, mAlo, mB, mBlo;
   e = make_panel_map(&mA, pa, P.elem, P.d_pad, P.q_pad, TC_M);
-  if (e == cudaSuccess) e = make_panel_map(&mB, C.pb, P.elem, P.d_pad, P.r_pad, P.N);
+  if (e == cudaSuccess) e = make_panel_map(&mB, cand_pb, P.elem, P.d_pad, P.r_pad, P.N);
   if (e != cudaSuccess) return e;
   mAlo = mA;
   mBlo = mB;
   if (P.fmt == 2) {
     e = make_panel_map(&mAlo, pa_lo, P.elem, P.d_pad, P.q_pad, TC_M);
-    if (e == cudaSuccess) e = make_panel_map(&mBlo, C.pb_lo, P.elem, P.d_pad, P.r_pad, P.N);
+    if (e == cudaSuccess) e = make_panel_map(&mBlo, cand_pb_lo, P.elem, P.d_pad, P.r_pad, P.N);
     if (e != cudaSuccess) return e;
   }
   TcParams tp{};
@@ -1221,10 +1296,12 @@ cudaError_t tc_run_prepared(const TcPlan &P, const TcCand &C, int nq, int d, int
   tp.status = status;
   tp.dbg = dbg;
   tp.dbg_ld = dbg_ld;
-  tp.dbg_ncols = nc;
+  tp.dbg_ncols = C.nc;
   tp.counters = counters;
+  tp.dQ = dQ;
+  tp.rowmap = rowmap;
   dim3 grid(P.qtiles, P.S);
-  mark("tc_knn", true);
+  mark(n_knn, true);
   if (P.fmt == 0) {
     e = cudaFuncSetAttribute(tc_knn<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, P.smem);
     if (e == cudaSuccess) tc_knn<0><<<grid, NTHREADS, P.smem, st>>>(mA, mAlo, mB, mBlo, tp);
@@ -1236,7 +1313,7 @@ cudaError_t tc_run_prepared(const TcPlan &P, const TcCand &C, int nq, int d, int
     if (e == cudaSuccess) tc_knn<2><<<grid, NTHREADS, P.smem, st>>>(mA, mAlo, mB, mBlo, tp);
   }
   if (e == cudaSuccess) e = cudaGetLastError();
-  mark("tc_knn", false, 1);
+  mark(n_knn, false, 1);
   if (e != cudaSuccess) return e;
 
   RerankParams rp{};
@@ -1248,22 +1325,114 @@ cudaError_t tc_run_prepared(const TcPlan &P, const TcCand &C, int nq, int d, int
   rp.fallback_list = reinterpret_cast<int *>(base + P.o_fbl);
   rp.fallback_count = fbc;
   rp.counters = counters;
-  FallbackParams fp{};
-  fp.k = k; fp.d = d; fp.nc = nc; fp.Xq = Xq; fp.Xq2 = Xq2; fp.Xc = C.Xc; fp.Xc2 = C.Xc2;
-  fp.qidx = qidx; fp.cidx = C.cidx; fp.nrows_c = C.nrows_c; fp.D = D; fp.I = I; fp.ldD = ldD;
-  fp.list = rp.fallback_list; fp.count = fbc;
+  rp.dQ = dQ;
+  rp.rowmap = rowmap;
   const int rb = (nq + 7) / 8;
-  mark("tc_rerank", true);
+  mark(n_rr, true);
   switch (P.kp) {
-    case 32: tc_rerank<1><<<rb, 256, 0, st>>>(rp); tc_fallback<1><<<148, 256, 0, st>>>(fp); break;
-    case 64: tc_rerank<2><<<rb, 256, 0, st>>>(rp); tc_fallback<2><<<148, 256, 0, st>>>(fp); break;
-    case 128: tc_rerank<4><<<rb, 256, 0, st>>>(rp); tc_fallback<4><<<148, 256, 0, st>>>(fp); break;
-    case 256: tc_rerank<8><<<rb, 256, 0, st>>>(rp); tc_fallback<8><<<148, 256, 0, st>>>(fp); break;
+    case 32: tc_rerank<1><<<rb, 256, 0, st>>>(rp); break;
+    case 64: tc_rerank<2><<<rb, 256, 0, st>>>(rp); break;
+    case 128: tc_rerank<4><<<rb, 256, 0, st>>>(rp); break;
+    case 256: tc_rerank<8><<<rb, 256, 0, st>>>(rp); break;
     default: return cudaErrorInvalidValue;
   }
   e = cudaGetLastError();
-  mark("tc_rerank", false, 2);  // re-rank and fallback
+  mark(n_rr, false, 1);
   return e;
+}
+
+// Exact FP64 brute force for the queries (heap rows) listed at base + P.o_fbl.
+static cudaError_t tc_brute(const TcPlan &P, const TcCand &C, int d, int k, const float *Xq,
+                            const float *Xq2, const int *qidx, float *D, int *I, int ldD,
+                            char *base, cudaStream_t st, TraceHook hook, void *hook_ctx) {
+  using namespace tc;
+  FallbackParams fp{};
+  fp.k = k; fp.d = d; fp.nc = C.nc; fp.Xq = Xq; fp.Xq2 = Xq2; fp.Xc = C.Xc; fp.Xc2 = C.Xc2;
+  fp.qidx = qidx; fp.cidx = C.cidx; fp.nrows_c = C.nrows_c; fp.D = D; fp.I = I; fp.ldD = ldD;
+  fp.list = reinterpret_cast<const int *>(base + P.o_fbl);
+  fp.count = reinterpret_cast<const int *>(base + P.o_fbc);
+  if (hook) hook(hook_ctx, "tc_fallback", true, st, 0);
+  switch (P.kp) {
+    case 32: tc_fallback<1><<<148, 256, 0, st>>>(fp); break;
+    case 64: tc_fallback<2><<<148, 256, 0, st>>>(fp); break;
+    case 128: tc_fallback<4><<<148, 256, 0, st>>>(fp); break;
+    case 256: tc_fallback<8><<<148, 256, 0, st>>>(fp); break;
+    default: return cudaErrorInvalidValue;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (hook) hook(hook_ctx, "tc_fallback", false, st, 1);
+  return e;
+}
+
+cudaError_t tc_run_prepared(const TcPlan &P, const TcCand &C, int nq, int d, int k,
+                            const float *Xq, const float *Xq2, long long nrows_q,
+                            const int *qidx, float *D, int *I, int ldD, void *ws, int *status,
+                            float *dbg, long long dbg_ld, unsigned long long *counters,
+                            cudaStream_t st, TraceHook hook, void *hook_ctx) {
+  using namespace tc;
+  if (C.fmt != P.fmt || C.d_pad != P.d_pad || C.r_pad != P.r_pad) return cudaErrorInvalidValue;
+  char *base = static_cast<char *>(ws);
+  cudaError_t e = tc_pass(P, C, C.pb, C.pb_lo, nq, d, k, Xq, Xq2, nrows_q, qidx, nullptr,
+                          nullptr, D, I, ldD, base, status, dbg, dbg_ld, counters, st, hook,
+                          hook_ctx, false);
+  if (e != cudaSuccess) return e;
+  // Escalation: the queries whose log overflowed run again in the narrower format against the
+  // same candidates (their panels in that format: prepared with the candidates, or packed here
+  // only when some query overflowed), as a pass over the list of overflowed heap rows whose
+  // length stays on the device. What overflows there too goes to the FP64 brute force.
+  const TcPlan EP = P.esc_mode ? tc_plan_base(nq, C.nc, d, k, P.esc_mode, P.sms, false,
+                                              P.max_splits)
+                               : TcPlan{};
+  void *epb = nullptr, *epb_lo = nullptr;
+  if (EP.ok && C.efmt == EP.fmt) {
+    epb = C.epb;
+    epb_lo = C.epb_lo;
+  } else if (EP.ok && P.ecand_bytes) {
+    epb = base + P.o_ecand;
+    epb_lo = EP.fmt == 2 ? base + P.o_ecand + P.ecand_bytes / 2 : nullptr;
+    if (hook) hook(hook_ctx, "tc_escalate", true, st, 0);
+    tc_pack<<<(C.r_pad + 7) / 8, 256, 0, st>>>(EP.fmt, C.Xc, C.Xc2, d, EP.d_pad, C.nrows_c,
+                                              C.cidx, C.nc, C.r_pad, C.mu, C.mu2, 1, epb,
+                                              epb_lo, nullptr, nullptr, nullptr, nullptr,
+                                              status, nullptr, nullptr,
+                                              reinterpret_cast<int *>(base + P.o_fbc));
+    e = cudaGetLastError();
+    if (hook) hook(hook_ctx, "tc_escalate", false, st, 1);
+    if (e != cudaSuccess) return e;
+  }
+  if (!epb) return tc_brute(P, C, d, k, Xq, Xq2, qidx, D, I, ldD, base, st, hook, hook_ctx);
+  TcCand C2 = C;
+  C2.fmt = EP.fmt;
+  C2.elem = EP.elem;
+  C2.d_pad = EP.d_pad;
+  C2.pb = epb;
+  C2.pb_lo = epb_lo;
+  char *ebase = base + P.o_esc;
+  e = tc_pass(EP, C2, epb, epb_lo, nq, d, k, Xq, Xq2, nrows_q, qidx,
+              reinterpret_cast<const int *>(base + P.o_fbc),
+              reinterpret_cast<const int *>(base + P.o_fbl), D, I, ldD, ebase, status, nullptr,
+              0, nullptr, st, hook, hook_ctx, true);
+  if (e != cudaSuccess) return e;
+  return tc_brute(EP, C2, d, k, Xq, Xq2, qidx, D, I, ldD, ebase, st, hook, hook_ctx);
+}
+
+// Escalation panels of a prepared candidate set (kept with it, e.g. a serving engine's
+// resident set): the same rows in `mode`'s format, sharing shift, norms, bounds and ids.
+cudaError_t tc_cand_prepare_escalation(TcCand *C, void *mem, int mode, int *status,
+                                       cudaStream_t st) {
+  using namespace tc;
+  const CandLayout L = cand_layout(C->nc, C->d, mode);
+  if (L.r_pad != C->r_pad) return cudaErrorInvalidValue;
+  char *b = static_cast<char *>(mem);
+  const size_t one = al256((size_t)L.r_pad * L.d_pad * L.elem);
+  C->efmt = L.fmt;
+  C->epb = b;
+  C->epb_lo = L.fmt == 2 ? b + one : nullptr;
+  tc_pack<<<(C->r_pad + 7) / 8, 256, 0, st>>>(L.fmt, C->Xc, C->Xc2, C->d, L.d_pad, C->nrows_c,
+                                             C->cidx, C->nc, C->r_pad, C->mu, C->mu2, 1,
+                                             C->epb, C->epb_lo, nullptr, nullptr, nullptr,
+                                             nullptr, status, nullptr, nullptr, nullptr);
+  return cudaGetLastError();
 }
 
 }  // namespace gsknn

@@ -160,3 +160,55 @@ def test_tc_ties_and_duplicates_exact(oracle):
         Ds, Is = sorted_rows(D.astype(np.float64), I)
         assert np.array_equal(Is, Ie), mode
         assert np.array_equal(Ds, De), mode
+
+
+def _traced_run(mode, X, X2, alpha, beta, k):
+    """_run with the library's launch tracer on; returns (D, I, kernel brackets seen)."""
+    import json
+    L = G.lib()
+    buf = ctypes.create_string_buffer(1 << 16)
+    L.gsknn_trace_read(buf, len(buf))
+    L.gsknn_trace_enable(1)
+    try:
+        D, I, _, _ = _run(mode, X, X2, alpha, beta, k, want_C=False)
+    finally:
+        L.gsknn_trace_enable(0)
+    L.gsknn_trace_read(buf, len(buf))
+    return D, I, json.loads(buf.value.decode() or "{}")
+
+
+def test_bf16_log_overflow_escalates_to_split_bf16(oracle):
+    """Clustered data at d = 64: the BF16 band holds most of a query's cluster, its logs
+    overflow, and those queries run again in split BF16 (the escalation pass) instead of the
+    FP64 brute force. Results stay the exact FP64 sets."""
+    N, d, k = 40000, 64, 32
+    X = W.gaussian_mixture_table(801, N, d, dtype=np.float32)
+    X2 = W.sq_norms(X)
+    alpha = W.permutation(802, N)[:30000].astype(np.int32)
+    beta = W.permutation(803, N)[:1000].astype(np.int32)
+    D, I, tr = _traced_run("bf16", X, X2, alpha, beta, k)
+    assert "tc_escalate" in tr, tr  # the escalation pass is launched (its work is on-device)
+    De, Ie = oracle.knn_exact(k, X, X2, alpha, X, X2, beta,
+                              np.full((1000, k), np.inf, dtype=np.float32),
+                              np.full((1000, k), -1, dtype=np.int32), clamp=True)
+    assert_same_sets(X, X2, beta, I, Ie, De)
+    assert_close(np.sort(D.astype(np.float64), axis=1), De)
+    assert is_maxheap(D)
+
+
+@pytest.mark.parametrize("mode", ["tf32", "bf16", "bf16x3"])
+def test_all_equal_points_go_to_brute_force(oracle, mode):
+    """Every candidate at the same distance: every band overflows in every format, so the
+    queries end in the FP64 brute force, which keeps the lowest ids (the tie rule)."""
+    N, d, k = 3000, 32, 16
+    X = np.tile(W.uniform(804, (1, d)).astype(np.float32), (N, 1))
+    X[:5] += 1.0  # a few distinct points, far away
+    X2 = W.sq_norms(X)
+    alpha = W.permutation(805, N)[:2500].astype(np.int32)
+    beta = W.permutation(806, N)[:200].astype(np.int32)
+    D, I, _ = _traced_run(mode, X, X2, alpha, beta, k)
+    De, Ie = oracle.knn_exact(k, X, X2, alpha, X, X2, beta,
+                              np.full((200, k), np.inf, dtype=np.float32),
+                              np.full((200, k), -1, dtype=np.int32), clamp=True)
+    Ds, Is = sorted_rows(D.astype(np.float64), I)
+    assert np.array_equal(Is, Ie)
