@@ -972,14 +972,16 @@ def serving_form(L, G, W, dev, args):
     lat, queue, rows, first, wall = run_stream(n, args.serve_rate, 56)
     n_light = max(1, n // 2)
     lat_l, queue_l, rows_l, first_l, wall_l = run_stream(n_light, args.serve_rate / 3.0, 57)
+    srv_mode, srv_probe = srv.mode, {k: round(v, 3) for k, v in srv.probe_ms.items()}
     srv.close()
     evals = float(ms.sum()) * nref
     res = {
         "workload": (f"serving: resident refs={nref} d={d} U[0,1); {n} requests, Poisson "
                      f"{args.serve_rate:g}/s, m log-uniform [1,4096] (mean {ms.mean():.0f}), "
                      f"k in {{8,16,64}}"),
-        "dtype": f"f32 inputs; {args.serve_mode} tensor distances + fp64 re-rank (exact top-k)"
-                 + (" [auto = split bf16 here]" if args.serve_mode == "auto" else ""),
+        "dtype": (f"f32 inputs; {MODE_NAMES.get(srv_mode, srv_mode)} tensor distances + fp64 "
+                  f"re-rank (exact top-k)" + (f" [auto: probe batch {srv_probe}]"
+                                               if args.serve_mode == "auto" else "")),
         "latency_ms": summary(lat, queue, ms),
         "value": evals / wall, "unit": "distance-evals/s",
         "wall_s": wall, "mean_batch_rows": float(np.mean(rows)),

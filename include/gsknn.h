@@ -300,8 +300,11 @@ void gsknn_batch_forget_tuning(void);
  * No counterpart in the reference (a caller would run sgsknn once per request).
  *
  * gsknn_serve_create prepares the nref x d float reference set R (device pointer, with norms
- * R2) once: packed for the tensor cores (mode AUTO / TF32 / BF16 / BF16X3; AUTO = split BF16
- * where its tiles fit, else TF32) and resident until destroy. Each request is m query rows
+ * R2) once: packed for the tensor cores (mode AUTO / TF32 / BF16 / BF16X3) and resident until
+ * destroy. In BF16 or TF32 the set is also packed in split BF16, where queries whose re-rank
+ * band overflows finish. AUTO prepares BF16 with those split panels, times one probe batch of
+ * resident points (k = max_k) both in BF16 and in split BF16 alone, and serves in the faster
+ * (TF32 where split tiles do not fit); gsknn_serve_mode reports the choice. Each request is m query rows
  * (host memory, copied at submit) and a k <= max_k; its result is the exact FP64 top-k of every
  * query against R (ties to the lower id), as a heap of m rows x k (descending rows) that stays
  * on the device until the request is released.
@@ -339,6 +342,9 @@ int gsknn_serve_set_slice(gsknn_serve_t *eng, int rows);
 /* While paused (nonzero) the dispatcher starts no new batch; requests still queue. Running
  * batches finish. Resuming dispatches everything queued in arrival order. */
 int gsknn_serve_pause(gsknn_serve_t *eng, int paused);
+/* The arithmetic the engine serves in (GSKNN_MODE_TF32 / BF16 / BF16X3) and, after an AUTO
+ * choice, the probe batch's milliseconds in BF16 and in split BF16 (0 when not probed). */
+int gsknn_serve_mode(gsknn_serve_t *eng, double *probe_bf16_ms, double *probe_bf16x3_ms);
 void gsknn_serve_destroy(gsknn_serve_t *eng);
 
 /* ---- Streaming form: the batching form for point sets beyond HBM ---------------------------

@@ -199,6 +199,10 @@ struct Engine {
   TcCand C{};
   void *cand_mem = nullptr;
   void *ecand_mem = nullptr;  // the resident set's panels in the escalation format
+  // The resident set as batches use it: C itself, or (when the engine measured the escalation
+  // format faster) C's escalation panels run as the main format.
+  TcCand Crun{};
+  double probe_ms[2] = {0.0, 0.0};  // AUTO: probe batch in BF16 (+escalation) and split BF16
   int *cidx = nullptr, *status = nullptr;
   char *arena_mem = nullptr;
   std::unique_ptr<serve::Arena> arena;
@@ -303,7 +307,7 @@ static cudaError_t launch_batch(Engine *E, gs::Slot &s) {
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if (E->trace) gs::stamp<<<1, 1, 0, st>>>(stamps + 1);
-  e = tc_run_prepared(P, E->C, rows, E->d, kb, s.Xq, s.Xq2, E->max_q, s.qidx, s.Db, s.Ib, kb,
+  e = tc_run_prepared(P, E->Crun, rows, E->d, kb, s.Xq, s.Xq2, E->max_q, s.qidx, s.Db, s.Ib, kb,
                       s.ws, s.status, nullptr, 0, nullptr, st, nullptr, nullptr);
   if (e != cudaSuccess) return e;
   dim3 blk(32, 8);
@@ -458,6 +462,64 @@ static void completion_loop(Engine *E) {
 // Rows per batch that keep one batch near 3 ms of tensor work on one B200: the exact forms
 // measured about 1.5e12 evals/s at d = 64 and 8.6e11 at d = 128, i.e. about 3e11 eval-dims per
 // 3 ms. Whole query tiles (128 rows), at least one, at most max_batch_queries.
+// The resident set's escalation panels as a main-format candidate set of their own.
+static gsknn::TcCand escalation_as_main(const gsknn::TcCand &C, int esc_mode) {
+  gsknn::TcCand S = C;
+  const gsknn::TcPlan P = gsknn::tc_plan(128, C.nc, C.d, 1, esc_mode, 148, false, 148);
+  S.fmt = C.efmt;
+  S.elem = C.efmt == 0 ? 4 : 2;
+  S.d_pad = P.d_pad;
+  S.pb = C.epb;
+  S.pb_lo = C.epb_lo;
+  S.efmt = -1;
+  S.epb = S.epb_lo = nullptr;
+  return S;
+}
+
+// Times one probe batch (the first min(max_q, 1024) resident points as queries, k = max_k) in
+// the prepared mode with escalation and in the escalation mode alone; keeps the faster (second
+// of two runs each, on slot 0's buffers). Returns false when a probe call fails.
+static bool probe_modes(Engine *E, int esc) {
+  using namespace gsknn;
+  gs::Slot &s = E->slots[0];
+  const int rows = std::min(E->max_q, 1024), kb = E->max_k;
+  const TcCand Cesc = escalation_as_main(E->C, esc);
+  const int modes[2] = {E->mode, esc};
+  const TcCand *cands[2] = {&E->C, &Cesc};
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) return false;
+  bool ok = true;
+  for (int m = 0; m < 2 && ok; m++) {
+    const TcPlan P = tc_plan(rows, E->nref, E->d, kb, modes[m], E->sms, false, E->sms);
+    if (!P.ok || P.bytes > E->ws_bytes) {
+      E->probe_ms[m] = 1e30;
+      continue;
+    }
+    float ms = 0.f;
+    for (int rep = 0; rep < 2 && ok; rep++) {
+      const long long n = (long long)rows * kb;
+      gs::fill_heap<<<(unsigned)((n + 255) / 256), 256, 0, s.st>>>(s.Db, s.Ib, n);
+      ok = cudaEventRecord(a, s.st) == cudaSuccess &&
+           tc_run_prepared(P, *cands[m], rows, E->d, kb, E->C.Xc, E->C.Xc2, E->nref, s.qidx,
+                           s.Db, s.Ib, kb, s.ws, s.status, nullptr, 0, nullptr, s.st, nullptr,
+                           nullptr) == cudaSuccess &&
+           cudaEventRecord(b, s.st) == cudaSuccess &&
+           cudaEventSynchronize(b) == cudaSuccess && cudaEventElapsedTime(&ms, a, b) ==
+                                                        cudaSuccess;
+    }
+    E->probe_ms[m] = ms;
+  }
+  int st = 0;
+  if (ok) ok = cudaMemcpy(&st, s.status, 4, cudaMemcpyDeviceToHost) == cudaSuccess && st == 0;
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (ok && E->probe_ms[1] < E->probe_ms[0]) {
+    E->mode = esc;
+    E->Crun = Cesc;
+  }
+  return ok;
+}
+
 static int auto_slice(const Engine *E) {
   const double rows = 3.0e11 / ((double)E->nref * (double)E->d);
   int s = (int)(rows / 128.0) * 128;
@@ -475,9 +537,14 @@ gsknn_serve_t *gsknn_serve_create(const float *R, const float *R2, int nref, int
     serr(GSKNN_ERR_ARG, "gsknn_serve_create: invalid argument");
     return nullptr;
   }
-  if (mode == GSKNN_MODE_AUTO)
+  // AUTO prepares the resident set in BF16 with split-BF16 escalation panels (queries whose
+  // BF16 band overflows finish in split BF16), then measures a probe batch both ways -- BF16
+  // with escalation, and split BF16 alone on the escalation panels -- and serves with the
+  // faster. Where split tiles do not fit, TF32.
+  const bool auto_mode = mode == GSKNN_MODE_AUTO;
+  if (auto_mode)
     mode = tc_plan(max_batch_queries, nref, d, max_k, GSKNN_TC_BF16X3, 148, false, 148).ok
-               ? GSKNN_MODE_BF16X3
+               ? GSKNN_MODE_BF16
                : GSKNN_MODE_TF32;
   if (mode < GSKNN_MODE_TF32 || mode > GSKNN_MODE_BF16X3) {
     serr(GSKNN_ERR_ARG, "gsknn_serve_create: mode must be AUTO, TF32, BF16 or BF16X3");
@@ -492,7 +559,9 @@ gsknn_serve_t *gsknn_serve_create(const float *R, const float *R2, int nref, int
   cudaGetDevice(&dev);
   E->device = dev;
   cudaDeviceGetAttribute(&E->sms, cudaDevAttrMultiProcessorCount, dev);
-  // query-side workspace: the largest plan over batch sizes (whole query tiles) and k
+  // query-side workspace: the largest plan over batch sizes (whole query tiles) and k, in the
+  // prepared mode and (AUTO) in the escalation mode run alone
+  const int esc = tc_escalation_mode(E->max_q, nref, d, max_k, mode, E->sms);
   for (int kk = 1; kk <= max_k; kk++)
     for (int q = 128; q < E->max_q + 128; q += 128) {
       const TcPlan P = tc_plan(std::min(q, E->max_q), nref, d, kk, mode, E->sms, false, E->sms);
@@ -501,11 +570,14 @@ gsknn_serve_t *gsknn_serve_create(const float *R, const float *R2, int nref, int
         return nullptr;
       }
       E->ws_bytes = std::max(E->ws_bytes, P.bytes);
+      if (auto_mode && esc) {
+        const TcPlan P2 = tc_plan(std::min(q, E->max_q), nref, d, kk, esc, E->sms, false, E->sms);
+        if (P2.ok) E->ws_bytes = std::max(E->ws_bytes, P2.bytes);
+      }
     }
   const size_t cb = tc_cand_bytes(nref, d, mode);
   // queries whose band log overflows in this format run again in a narrower one: its panels of
   // the resident set are prepared once, beside the first
-  const int esc = tc_escalation_mode(E->max_q, nref, d, max_k, mode, E->sms);
   bool ok = (!esc || cudaMalloc(&E->ecand_mem, tc_cand_panel_bytes(nref, d, esc)) ==
                          cudaSuccess) &&
             cudaMalloc(&E->cand_mem, cb) == cudaSuccess &&
@@ -565,6 +637,12 @@ gsknn_serve_t *gsknn_serve_create(const float *R, const float *R2, int nref, int
     gsknn_serve_destroy(reinterpret_cast<gsknn_serve_t *>(E.release()));
     return nullptr;
   }
+  E->Crun = E->C;
+  if (auto_mode && esc && !probe_modes(E.get(), esc)) {
+    serr(GSKNN_ERR_CUDA, "gsknn_serve_create: the probe batch failed");
+    gsknn_serve_destroy(reinterpret_cast<gsknn_serve_t *>(E.release()));
+    return nullptr;
+  }
   E->slice = auto_slice(E.get());
   E->trace = std::getenv("GSKNN_SERVE_TRACE") != nullptr;
   for (auto &sl : E->slots)
@@ -578,6 +656,14 @@ gsknn_serve_t *gsknn_serve_create(const float *R, const float *R2, int nref, int
   raw->dispatcher = std::thread(dispatcher_loop, raw);
   set_status(GSKNN_OK, nullptr);
   return reinterpret_cast<gsknn_serve_t *>(raw);
+}
+
+int gsknn_serve_mode(gsknn_serve_t *eng, double *probe_bf16_ms, double *probe_bf16x3_ms) {
+  Engine *E = reinterpret_cast<Engine *>(eng);
+  if (!E) return -GSKNN_ERR_ARG;
+  if (probe_bf16_ms) *probe_bf16_ms = E->probe_ms[0];
+  if (probe_bf16x3_ms) *probe_bf16x3_ms = E->probe_ms[1];
+  return E->mode;
 }
 
 long long gsknn_serve_submit(gsknn_serve_t *eng, const float *Q, int m, int k) {

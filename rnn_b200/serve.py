@@ -44,6 +44,10 @@ class Server:
             raise G.GsknnError(L.gsknn_last_error(), G.last_error())
         self._h = h
         self._shape = {}
+        L.gsknn_serve_mode.argtypes = [vp, vp, vp]
+        a, b = ctypes.c_double(0.0), ctypes.c_double(0.0)
+        self.mode = L.gsknn_serve_mode(h, ctypes.byref(a), ctypes.byref(b))
+        self.probe_ms = {"bf16": a.value, "bf16x3": b.value}
         self.slice_rows = self.set_slice(slice_rows)
 
     def submit(self, Q: np.ndarray, k: int) -> int:
