@@ -311,6 +311,22 @@ __device__ __forceinline__ void epi_defer(float dp, bool ins, float (&pend)[PEND
   np += ins ? 1 : 0;
 }
 
+// One candidate of the exact slow path: log it (when `act` and under the threshold) and, for
+// heap owners, defer its heap insert. Branch-free: every lane of the warp runs it, with
+// predicates instead of divergent branches.
+__device__ __forceinline__ void epi_candidate(EpiState &s, float v, uint32_t id, bool act,
+                                              uint2 *lg, int logcap, bool owner,
+                                              float (&pend)[PEND], int &np) {
+  const float dp = v + s.qn;
+  const bool take = act && dp <= s.thr;
+  s.n_ev += take ? 1u : 0u;
+  const bool room = s.cnt < logcap;
+  if (take && !s.ovf && room) lg[s.cnt] = make_uint2(__float_as_uint(dp), id);
+  s.cnt += (take && !s.ovf && room) ? 1 : 0;
+  s.ovf |= (take && !room) ? 1 : 0;
+  epi_defer(dp, take && owner && dp < s.root, pend, np);
+}
+
 // Apply the deferred inserts (all lanes of the warp together, so their sift-downs overlap),
 // publish the new k-th to the other splits and tighten the threshold.
 __device__ __forceinline__ void epi_flush(EpiState &s, float *heap, int row, int k,
@@ -569,6 +585,53 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     // of the candidates seen (one real candidate per entry), so its root still bounds the k-th
     // smallest approximate distance from above, and every candidate within 2E of the final
     // k-th stays under the threshold and is logged.
+    // Exact slow part, for the owner's first chunks while its heap is still filling (a chunk
+    // then often holds several values under the root, and the chunk minimum alone would leave
+    // the threshold loose): a warp-convergent pass in which every lane with pending candidates
+    // logs one of them per iteration (selected from its registers by index) and defers its
+    // heap insert.
+    auto slow_exact = [&](const uint32_t (&r)[32], size_t cbase, int c0) {
+      if (__any_sync(FULL_MASK, s.cnt > p.logcap - 32)) {
+        if (s.cnt > p.logcap - 32 && !s.ovf) {
+          s.cnt = log_compact(lg, s.cnt, s.thr);
+          if (s.cnt > p.logcap - 32) {
+            s.ovf = 1;
+            refresh_threshold(s);
+          }
+        }
+      }
+      // pass mask as an OR tree (depth 5), built by every lane
+      uint32_t m16[16];
+#pragma unroll
+      for (int j = 0; j < 16; j++)
+        m16[j] = (__uint_as_float(r[2 * j]) <= s.Tv ? 1u << (2 * j) : 0u) |
+                 (__uint_as_float(r[2 * j + 1]) <= s.Tv ? 1u << (2 * j + 1) : 0u);
+#pragma unroll
+      for (int w = 8; w >= 1; w >>= 1)
+#pragma unroll
+        for (int j = 0; j < w; j++) m16[j] = m16[2 * j] | m16[2 * j + 1];
+      uint32_t mask = m16[0];
+      s.n_sc++;
+      while (__any_sync(FULL_MASK, mask != 0)) {
+        s.n_it++;
+        const bool act = mask != 0;
+        const int i = (__ffs(mask) - 1) & 31;
+        mask &= mask - 1;
+        // v[i] for a runtime i: a 5-level select tree on the bits of i
+        float t16[16];
+#pragma unroll
+        for (int j = 0; j < 16; j++) t16[j] = __uint_as_float((i & 16) ? r[j + 16] : r[j]);
+#pragma unroll
+        for (int w = 8, bit = 8; w >= 1; w >>= 1, bit >>= 1)
+#pragma unroll
+          for (int j = 0; j < w; j++) t16[j] = (i & bit) ? t16[j + w] : t16[j];
+        epi_candidate(s, t16[0], (uint32_t)(cbase + c0 + i), act && valid, lg, p.logcap, owner,
+                      pend, np);
+        if (__any_sync(FULL_MASK, np == PEND)) {
+          if (owner) epi_flush(s, heap, row, p.k, pend, np, ksh);
+        }
+      }
+    };
     auto slow = [&](const uint32_t (&r)[32], float mn, size_t cbase, int c0) {
       // a chunk appends at most 32 entries per lane: make room first, all lanes together
       if (__any_sync(FULL_MASK, s.cnt > p.logcap - 32)) {
@@ -595,8 +658,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       s.n_ev += (unsigned)(cnt - s.cnt);
       s.cnt = cnt;
       if (owner) {
-        const float dm = mn + s.qn;  // NaN when every column is padding: never inserted
-        epi_defer(dm, dm < s.root, pend, np);
+        // NaN when every column is padding: never inserted. Padding rows (past the last query)
+        // insert nothing either: their heap root would reach query 0's shared bound.
+        const float dm = mn + s.qn;
+        epi_defer(dm, valid && dm < s.root, pend, np);
         if (__any_sync(FULL_MASK, np == PEND)) epi_flush(s, heap, row, p.k, pend, np, ksh);
       }
     };
@@ -605,6 +670,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     unsigned sh_next = valid ? __ldcg(ksh) : 0xFFFFFFFFu;
     const long long t_start = p.counters ? clock64() : 0;
     long long w_tfull = 0;
+    // the owner's first 2k chunks take the exact slow path: past them, a chunk rarely holds two
+    // values under the row's root, so its minimum alone keeps the heap (nearly) exact
+    int nchunk = 0;
+    const int early_chunks = 2 * p.k;
     for (int lt = 0; lt < ntile && !failed; lt++) {
       const int b = lt & 1, c = lt % CN_SLOTS;
       const uint32_t use = (uint32_t)(lt >> 1), cuse = (uint32_t)(lt / CN_SLOTS);
@@ -660,8 +729,16 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             dbg_write(ra, cbase, c0);
             dbg_write(rb, cbase, c0 + 32);
           }
-          if (__any_sync(FULL_MASK, ma <= s.Tv)) slow(ra, ma, cbase, c0);
-          if (__any_sync(FULL_MASK, mb <= s.Tv)) slow(rb, mb, cbase, c0 + 32);
+          const bool exact = owner && nchunk < early_chunks;  // warp-uniform
+          if (__any_sync(FULL_MASK, ma <= s.Tv)) {
+            if (exact) slow_exact(ra, cbase, c0);
+            else slow(ra, ma, cbase, c0);
+          }
+          if (__any_sync(FULL_MASK, mb <= s.Tv)) {
+            if (exact) slow_exact(rb, cbase, c0 + 32);
+            else slow(rb, mb, cbase, c0 + 32);
+          }
+          nchunk += 2;
         } else {
           uint32_t ra[32];
           __syncwarp();
@@ -675,7 +752,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           }
           const float ma = fast(ra, cnt, c0);
           if (p.dbg && valid) dbg_write(ra, cbase, c0);
-          if (__any_sync(FULL_MASK, ma <= s.Tv)) slow(ra, ma, cbase, c0);
+          if (__any_sync(FULL_MASK, ma <= s.Tv)) {
+            if (owner && nchunk < early_chunks) slow_exact(ra, cbase, c0);
+            else slow(ra, ma, cbase, c0);
+          }
+          nchunk += 1;
         }
       }
     }

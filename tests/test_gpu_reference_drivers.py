@@ -41,9 +41,9 @@ def test_reference_driver(case):
     out = subprocess.run([path, str(m), str(n), str(d), str(r)], capture_output=True, text=True,
                          timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
-    lines = out.stdout.strip().splitlines()
+    lines = [ln.strip() for ln in out.stdout.strip().splitlines()]
     assert lines and re.search(r"GFLOPS;$", lines[-1]), out.stdout[-2000:]
-    assert f"{m:5d}, {n:5d}, {d:5d}, {r:5d}," in lines[-1]
+    assert re.match(rf"{m},\s+{n},\s+{d},\s+{r},", lines[-1]), lines[-1]
     assert not any(ln.strip() == "bug" for ln in lines)
     worst = 0.0
     for ln in lines[:-1]:
