@@ -106,6 +106,11 @@ def parse():
                     help="arithmetic of the serving engine (a tensor-core mode or auto)")
     ap.add_argument("--serve-rate", type=float, default=150.0,
                     help="mean request arrival rate (requests/s, Poisson)")
+    ap.add_argument("--kernel-case", default=None,
+                    choices=["config1", "large_k", "tc_q8192", "batch_small", "serve_one",
+                             "fp32_q8192"],
+                    help="one small run of one path, for per-kernel profiling: warm-up call, "
+                         "then the profiled call")
     ap.add_argument("--cpu-worker", default=None, help=argparse.SUPPRESS)
     return ap.parse_args()
 
@@ -1076,6 +1081,74 @@ def e2e_host(L, G, p, beta_h, args):
 
 
 
+
+def kernel_case(name: str) -> dict:
+    """One small invocation of one path (a warm-up call, then the call to profile), so that an
+    ncu capture of any of the library's kernels can be taken on a small case:
+      config1     dgsknn FP64 (pack_panels, fused_knn_simt<double>, finalize_heap)
+      large_k     k = 600 float (dist_block, select_rows)
+      tc_q8192    split BF16 on 8,192 headline queries (tc_pack, tc_knn, tc_rerank)
+      fp32_q8192  plain FP32 on 8,192 headline queries (fused_knn_simt<float>)
+      batch_small one pass of 8 trees over 262,144 mixture points (batch_pack, batch_knn_simt,
+                  batch_merge)
+      serve_one   one 512-row request against 1,048,576 resident points (query_norms,
+                  scatter, the tensor-core kernels)"""
+    import torch
+    from rnn_b200 import gsknn as G
+    from rnn_b200 import workloads as W
+    dev = torch.device("cuda:0")
+    torch.cuda.set_device(dev)
+    t = time.perf_counter()
+
+    def dev_call(X, X2, alpha, beta, k, mode=0, reps=2):
+        Xd, X2d = torch.from_numpy(X).to(dev), torch.from_numpy(X2).to(dev)
+        a, b = torch.from_numpy(alpha).to(dev), torch.from_numpy(beta).to(dev)
+        D = torch.empty((beta.size, k), dtype=Xd.dtype, device=dev)
+        I = torch.empty((beta.size, k), dtype=torch.int32, device=dev)
+        G.set_mode(mode)
+        for _ in range(reps):
+            D.fill_(float("inf"))
+            I.fill_(-1)
+            G.knn_device(Xd, X2d, a, Xd, X2d, b, D, I)
+        torch.cuda.synchronize()
+        G.set_mode(0)
+
+    if name == "config1":
+        p, _ = W.config1(1)
+        dev_call(p.X, p.X2, p.alpha, p.beta, p.k)
+    elif name == "large_k":
+        p = W.config2(n_queries=2048, n_refs=65536, k=600)
+        dev_call(p.X, p.X2, p.alpha, p.beta, p.k)
+    elif name in ("tc_q8192", "fp32_q8192"):
+        p = W.config2()
+        beta = np.ascontiguousarray(p.beta[:8192])
+        dev_call(p.X, p.X2, p.alpha, beta, p.k, mode=1 if name == "fp32_q8192" else 0)
+    elif name == "batch_small":
+        from rnn_b200 import batch as B
+        p = W.config4(n_points=1 << 18, passes=1)
+        lv = B.rkdt_leaves(p.X, p.trees_per_pass, p.leaf_min, p.leaf_max, seed=p.tree_seed)
+        Xd, X2d = torch.from_numpy(p.X).to(dev), torch.from_numpy(p.X2).to(dev)
+        D = torch.full((p.N, p.k), float("inf"), device=dev)
+        I = torch.full((p.N, p.k), -1, dtype=torch.int32, device=dev)
+        job = B.BatchJob(Xd, X2d, D, I, p.k, p.trees_per_pass, p.leaf_min, shape=2,
+                         stream=torch.cuda.current_stream(dev))
+        for _ in range(2):
+            job.run_pass(lv)
+        job.sync()
+    elif name == "serve_one":
+        from rnn_b200 import serve as SV
+        R = W.uniform_table(61, 1 << 20, 128, np.float32)
+        Rd = torch.from_numpy(R).to(dev)
+        R2d = torch.from_numpy(W.sq_norms(R)).to(dev)
+        srv = SV.Server(Rd, R2d, mode=0, max_batch_queries=1024, max_k=64, slots=1)
+        Q = W.uniform_table(62, 512, 128, np.float32)
+        for _ in range(2):
+            rid = srv.submit(Q, 64)
+            srv.wait(rid)
+            srv.release(rid)
+        srv.close()
+    return {"kernel_case": name, "seconds": time.perf_counter() - t}
+
 def summarize(out: dict) -> dict:
     """Compact figures of every leg, placed last in the JSON line so that a reader keeping only
     the tail of the line still has them."""
@@ -1137,6 +1210,9 @@ def main():
     args = parse()
     if args.cpu_worker:
         cpu_worker(args.cpu_worker)
+        return
+    if args.kernel_case:
+        print(json.dumps(kernel_case(args.kernel_case)), flush=True)
         return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(256) pack_panels(
 //    the tile body is simt_block (knn_simt_body.cuh)
 // ------------------------------------------------------------------------------------------
 template <class C, int METRIC>
-__global__ void __launch_bounds__(C::NTHR) fused_knn_simt(SimtArgs<typename C::type> a) {
+__global__ void __launch_bounds__(C::NTHR, C::MINB) fused_knn_simt(SimtArgs<typename C::type> a) {
   using T = typename C::type;
   extern __shared__ __align__(128) unsigned char smem[];
   const int qt = blockIdx.x, split = blockIdx.y;
@@ -188,7 +188,7 @@ static cudaError_t run_simt(const SimtArgs<typename C::type> &a, int qtiles, int
 // Tile configurations per (precision, list size). Float: 8x8 per thread, 128 queries x 128
 // candidates per CTA (64 queries for the larger lists); double: 4x8 per thread.
 template <typename T, int KP> struct SimtPick;
-template <> struct SimtPick<float, 32> { using C = SimtCfg<float, 32, 2, 2, 4, 2, 16, 3>; };
+template <> struct SimtPick<float, 32> { using C = SimtCfg<float, 32, 2, 2, 4, 2, 16, 2, 2>; };
 template <> struct SimtPick<float, 64> { using C = SimtCfg<float, 64, 2, 2, 4, 2, 16, 3>; };
 template <> struct SimtPick<float, 128> { using C = SimtCfg<float, 128, 2, 2, 2, 4, 16, 3>; };
 template <> struct SimtPick<float, 256> { using C = SimtCfg<float, 256, 2, 2, 2, 4, 16, 3>; };

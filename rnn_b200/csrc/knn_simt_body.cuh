@@ -18,10 +18,12 @@
 
 namespace gsknn {
 
-template <typename T, int KP_, int GM, int GN, int WQ_, int WR_, int DK_, int NSTAGE_>
+template <typename T, int KP_, int GM, int GN, int WQ_, int WR_, int DK_, int NSTAGE_,
+          int MINB_ = 1>
 struct SimtCfg {
   using type = T;
   static constexpr int KP = KP_, DK = DK_, NSTAGE = NSTAGE_, WQ = WQ_, WR = WR_;
+  static constexpr int MINB = MINB_;  // resident CTAs per SM the launch bounds ask for
   static constexpr int TM = 4 * GM, TN = 4 * GN;
   static constexpr int WTQ = 16 * GM, WTR = 32 * GN;  // warp tile: 4 x 8 lanes
   static constexpr int BQ = WQ * WTQ, BR = WR * WTR;
