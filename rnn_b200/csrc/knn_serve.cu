@@ -488,7 +488,7 @@ static bool probe_modes(Engine *E, int esc) {
   const TcCand *cands[2] = {&E->C, &Cesc};
   cudaEvent_t a = nullptr, b = nullptr;
   if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) return false;
-  bool ok = true;
+  bool ok = cudaMemsetAsync(s.status, 0, sizeof(int), s.st) == cudaSuccess;
   for (int m = 0; m < 2 && ok; m++) {
     const TcPlan P = tc_plan(rows, E->nref, E->d, kb, modes[m], E->sms, false, E->sms);
     if (!P.ok || P.bytes > E->ws_bytes) {

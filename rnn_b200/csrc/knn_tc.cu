@@ -585,12 +585,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     // of the candidates seen (one real candidate per entry), so its root still bounds the k-th
     // smallest approximate distance from above, and every candidate within 2E of the final
     // k-th stays under the threshold and is logged.
-    // Exact slow part, for the owner's first chunks while its heap is still filling (a chunk
-    // then often holds several values under the root, and the chunk minimum alone would leave
-    // the threshold loose): a warp-convergent pass in which every lane with pending candidates
-    // logs one of them per iteration (selected from its registers by index) and defers its
+    // Slow part, for a chunk in which some lane has a candidate under its threshold: a
+    // warp-convergent pass in which every lane with pending candidates logs one of them per
+    // iteration (selected from its registers by index) and, for the row's owner, defers its
     // heap insert.
-    auto slow_exact = [&](const uint32_t (&r)[32], size_t cbase, int c0) {
+    auto slow = [&](const uint32_t (&r)[32], size_t cbase, int c0) {
       if (__any_sync(FULL_MASK, s.cnt > p.logcap - 32)) {
         if (s.cnt > p.logcap - 32 && !s.ovf) {
           s.cnt = log_compact(lg, s.cnt, s.thr);
@@ -632,48 +631,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         }
       }
     };
-    auto slow = [&](const uint32_t (&r)[32], float mn, size_t cbase, int c0) {
-      // a chunk appends at most 32 entries per lane: make room first, all lanes together
-      if (__any_sync(FULL_MASK, s.cnt > p.logcap - 32)) {
-        if (s.cnt > p.logcap - 32 && !s.ovf) {
-          s.cnt = log_compact(lg, s.cnt, s.thr);
-          if (s.cnt > p.logcap - 32) {
-            s.ovf = 1;
-            refresh_threshold(s);
-          }
-        }
-      }
-      s.n_sc++;
-      const float Tv = s.ovf ? -Num<float>::inf() : s.Tv;
-      const uint32_t pos = (uint32_t)(cbase + c0);
-      int cnt = s.cnt;
-#pragma unroll
-      for (int j = 0; j < 32; j++) {
-        const float v = __uint_as_float(r[j]);
-        if (v <= Tv) {
-          lg[cnt] = make_uint2(__float_as_uint(v + s.qn), pos + (uint32_t)j);
-          cnt++;
-        }
-      }
-      s.n_ev += (unsigned)(cnt - s.cnt);
-      s.cnt = cnt;
-      if (owner) {
-        // NaN when every column is padding: never inserted. Padding rows (past the last query)
-        // insert nothing either: their heap root would reach query 0's shared bound.
-        const float dm = mn + s.qn;
-        epi_defer(dm, valid && dm < s.root, pend, np);
-        if (__any_sync(FULL_MASK, np == PEND)) epi_flush(s, heap, row, p.k, pend, np, ksh);
-      }
-    };
     // what the query's other splits have found (all bits set = nothing yet); the load for the
     // next tile is issued a tile ahead so its latency hides behind the tile's work
     unsigned sh_next = valid ? __ldcg(ksh) : 0xFFFFFFFFu;
     const long long t_start = p.counters ? clock64() : 0;
     long long w_tfull = 0;
-    // the owner's first 2k chunks take the exact slow path: past them, a chunk rarely holds two
-    // values under the row's root, so its minimum alone keeps the heap (nearly) exact
-    int nchunk = 0;
-    const int early_chunks = 2 * p.k;
     for (int lt = 0; lt < ntile && !failed; lt++) {
       const int b = lt & 1, c = lt % CN_SLOTS;
       const uint32_t use = (uint32_t)(lt >> 1), cuse = (uint32_t)(lt / CN_SLOTS);
@@ -729,16 +691,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             dbg_write(ra, cbase, c0);
             dbg_write(rb, cbase, c0 + 32);
           }
-          const bool exact = owner && nchunk < early_chunks;  // warp-uniform
-          if (__any_sync(FULL_MASK, ma <= s.Tv)) {
-            if (exact) slow_exact(ra, cbase, c0);
-            else slow(ra, ma, cbase, c0);
-          }
-          if (__any_sync(FULL_MASK, mb <= s.Tv)) {
-            if (exact) slow_exact(rb, cbase, c0 + 32);
-            else slow(rb, mb, cbase, c0 + 32);
-          }
-          nchunk += 2;
+          if (__any_sync(FULL_MASK, ma <= s.Tv)) slow(ra, cbase, c0);
+          if (__any_sync(FULL_MASK, mb <= s.Tv)) slow(rb, cbase, c0 + 32);
         } else {
           uint32_t ra[32];
           __syncwarp();
@@ -752,11 +706,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           }
           const float ma = fast(ra, cnt, c0);
           if (p.dbg && valid) dbg_write(ra, cbase, c0);
-          if (__any_sync(FULL_MASK, ma <= s.Tv)) {
-            if (owner && nchunk < early_chunks) slow_exact(ra, cbase, c0);
-            else slow(ra, ma, cbase, c0);
-          }
-          nchunk += 1;
+          if (__any_sync(FULL_MASK, ma <= s.Tv)) slow(ra, cbase, c0);
         }
       }
     }
