@@ -946,8 +946,6 @@ __device__ __forceinline__ void load_heap_row(const float *D, const int *I, int 
 template <int E>
 __global__ void __launch_bounds__(256) tc_rerank(RerankParams p) {
   __shared__ uint32_t rr_stage[8][64];
-  constexpr int LIST = 256;  // pass 1's compacted list per warp
-  __shared__ float rr_list[8][LIST];
   const int lane = threadIdx.x & 31;
   const int q = blockIdx.x * 8 + (threadIdx.x >> 5);
   if (q >= (p.dQ ? *p.dQ : p.Q)) return;
@@ -968,47 +966,7 @@ __global__ void __launch_bounds__(256) tc_rerank(RerankParams p) {
   // candidate among the k smallest approximate distances was logged (its d' was below every
   // threshold in force), so this is the global approximate k-th, usually far below the bound T
   // the splits ended with.
-  // The entries at or under T are few (T is the k-th of a heap over part of the candidates):
-  // they are compacted into a per-warp list and sorted once. When more than LIST of them exist
-  // (or T is not finite) the running merge below finds the k-th instead.
-  bool done = false;
-  if (p.k <= LIST && T < Num<float>::inf()) {
-    float *lst = rr_list[threadIdx.x >> 5];
-    int n = 0;
-    for (int s = 0; s < p.S && n <= LIST; s++) {
-      const int cnt = p.logcnt[(size_t)s * p.Q + q];
-      const uint2 *lg = p.log + ((size_t)s * p.Q + q) * p.logcap;
-      for (int base = 0; base < cnt; base += 32) {
-        const int e = base + lane;
-        const float dv = e < cnt ? __uint_as_float(lg[e].x) : Num<float>::inf();
-        const bool take = dv <= T;
-        const unsigned m = __ballot_sync(FULL_MASK, take);
-        const int at = n + __popc(m & ((1u << lane) - 1u));
-        if (take && at < LIST) lst[at] = dv;
-        n += __popc(m);
-        if (n > LIST) break;
-      }
-    }
-    __syncwarp();
-    if (n >= p.k && n <= LIST) {
-      float v[LIST / 32];
-      uint32_t vi[LIST / 32];
-#pragma unroll
-      for (int e = 0; e < LIST / 32; e++) {
-        const int t = e * 32 + lane;
-        v[e] = t < n ? lst[t] : Num<float>::inf();
-        vi[e] = (uint32_t)t;
-      }
-      warp_sort<float, LIST / 32>(v, vi, lane);
-      float t = v[0];
-#pragma unroll
-      for (int e = 0; e < LIST / 32; e++)
-        if (e == (p.k - 1) / 32) t = v[e];
-      T = __shfl_sync(FULL_MASK, t, (p.k - 1) & 31);
-      done = true;
-    }
-  }
-  if (!done) {
+  {
     float kd[E];
     uint32_t ki[E];
 #pragma unroll
