@@ -342,7 +342,7 @@ int knn_device_simt(int nq, int nc, int d, int k, const T *Xq, const T *Xq2, lon
   const int nkc = (d + g.dk - 1) / g.dk;
   const int qtiles = (nq + g.bq - 1) / g.bq;
   const int rtiles = (nc + g.br - 1) / g.br;
-  const int S = choose_splits(qtiles, rtiles, sm_count());
+  const int S = choose_splits(qtiles, rtiles, sm_count() * std::max(1, g.minb));
   const int tps = (rtiles + S - 1) / S;
 
   size_t off = 0;

@@ -27,6 +27,7 @@ struct SimtGeom {
   int dk;      // dimension chunk
   size_t smem;
   int nthr;
+  int minb;  // resident CTAs per SM the kernel is built for
 };
 
 template <typename T>

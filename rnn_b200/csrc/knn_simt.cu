@@ -192,7 +192,7 @@ template <> struct SimtPick<float, 32> { using C = SimtCfg<float, 32, 2, 2, 4, 2
 template <> struct SimtPick<float, 64> { using C = SimtCfg<float, 64, 2, 2, 4, 2, 16, 3>; };
 template <> struct SimtPick<float, 128> { using C = SimtCfg<float, 128, 2, 2, 2, 4, 16, 3>; };
 template <> struct SimtPick<float, 256> { using C = SimtCfg<float, 256, 2, 2, 2, 4, 16, 3>; };
-template <> struct SimtPick<double, 32> { using C = SimtCfg<double, 32, 1, 2, 4, 2, 16, 3>; };
+template <> struct SimtPick<double, 32> { using C = SimtCfg<double, 32, 1, 2, 4, 2, 16, 2, 2>; };
 template <> struct SimtPick<double, 64> { using C = SimtCfg<double, 64, 1, 2, 4, 2, 16, 3>; };
 template <> struct SimtPick<double, 128> { using C = SimtCfg<double, 128, 1, 2, 4, 2, 8, 3>; };
 template <> struct SimtPick<double, 256> { using C = SimtCfg<double, 256, 1, 2, 2, 4, 8, 3>; };
@@ -207,7 +207,7 @@ SimtGeom simt_geometry(int k) {
   if (kp == KPV) {                                        \
     using C = typename SimtPick<T, KPV>::C;               \
     g.bq = C::BQ; g.br = C::BR; g.dk = C::DK;             \
-    g.smem = C::SMEM; g.nthr = C::NTHR;                   \
+    g.smem = C::SMEM; g.nthr = C::NTHR; g.minb = C::MINB; \
     return g;                                             \
   }
   GSKNN_GEOM(32) GSKNN_GEOM(64) GSKNN_GEOM(128) GSKNN_GEOM(256)
