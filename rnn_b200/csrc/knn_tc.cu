@@ -223,14 +223,9 @@ struct SmemLayout {
 
 constexpr int PEND = 8;  // heap inserts a lane may defer before the warp flushes them
 
-// Epilogue slow-path forms (`stg`):
-//   0  survivors found with a per-lane pass mask and read back through a select tree over the
-//      chunk's registers; deferred heap inserts in a register ring
-//   1  the same with each epilogue warp's 32 x 32 chunk values staged in shared memory (one
-//      load per survivor instead of the select tree) and the insert rings in shared memory
-//   2  grouped: warp votes on four 8-column group minima (computed by the fast filter), then
-//      on each column of a flagged group, with compile-time register indices throughout (no
-//      mask, no selection); insert rings in shared memory
+// `stg`: the epilogue's staging areas are in shared memory too -- each epilogue warp's 32 x 32
+// chunk values (so the slow path reads a value at a runtime column with one load, not a select
+// tree) and its deferred-insert rings.
 __host__ __device__ inline SmemLayout tc_smem_layout(int nkc, int a_terms, int b_terms, int N,
                                                      int NST, int k, int stg) {
   SmemLayout L;
@@ -247,9 +242,11 @@ __host__ __device__ inline SmemLayout tc_smem_layout(int nkc, int a_terms, int b
   off = (off + 15) & ~15u;
   L.stage_off = off;
   L.pend_off = off;
-  if (stg == 1) off += (uint32_t)NEPI * 32 * 32 * 4;
-  L.pend_off = off;
-  if (stg) off += (uint32_t)NEPI * PEND * 32 * 4;
+  if (stg) {
+    off += (uint32_t)NEPI * 32 * 32 * 4;
+    L.pend_off = off;
+    off += (uint32_t)NEPI * PEND * 32 * 4;
+  }
   off = (off + 7) & ~7u;
   L.bar_off = off;
   off += (uint32_t)(2 * NST + 5 + CN_SLOTS) * 8;  // full, empty, tfull[2], tempty[2], afull, cnfull
@@ -391,7 +388,7 @@ __device__ __forceinline__ void epi_flush(EpiState &s, float *heap, int row, int
   refresh_threshold(s);
 }
 
-template <int FMT, int STG>
+template <int FMT, bool STG>
 __global__ void __launch_bounds__(NTHREADS, 1)
     tc_knn(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tAlo,
            const __grid_constant__ CUtensorMap tB, const __grid_constant__ CUtensorMap tBlo,
@@ -552,9 +549,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     s.shared = Num<float>::inf();
     s.n_ev = s.n_ins = s.n_it = s.n_sc = 0;
     unsigned *ksh = p.kth_shared + (valid ? gq : 0);
-    using Ring = typename std::conditional<STG != 0, SmemRing, RegRing>::type;
+    using Ring = typename std::conditional<STG, SmemRing, RegRing>::type;
     Ring pend;
-    if constexpr (STG != 0) {
+    if constexpr (STG) {
       pend.p = reinterpret_cast<float *>(smem + L.pend_off) + (warp - 2) * PEND * 32;
       pend.lane = lane;
     }
@@ -596,7 +593,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     // Fast part of a 32-column chunk: d' - qn' (the v space) over the accumulator values in
     // place, and their minimum (a tree of depth 5). Two chunks' fast parts run back to back in
     // one basic block so their independent arithmetic overlaps.
-    auto fast = [&](uint32_t (&r)[32], const float *cnt, int c0, float (&gm)[4]) -> float {
+    auto fast = [&](uint32_t (&r)[32], const float *cnt, int c0) -> float {
       const float4 *cn4 = reinterpret_cast<const float4 *>(cnt + c0);
 #pragma unroll
       for (int j = 0; j < 8; j++) {
@@ -611,28 +608,16 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         r[4 * j + 2] = __float_as_uint(v2);
         r[4 * j + 3] = __float_as_uint(v3);
       }
-      if constexpr (STG == 2) {
-        // minima of the four 8-column groups (kept for the grouped slow path), then of those
+      // minimum: three-input tree of depth 4 (32 -> 11 -> 4 -> 1)
+      float m11[11];
 #pragma unroll
-        for (int g = 0; g < 4; g++) {
-          const uint32_t *x = r + 8 * g;
-          gm[g] = fmin3(fmin3(__uint_as_float(x[0]), __uint_as_float(x[1]), __uint_as_float(x[2])),
-                        fmin3(__uint_as_float(x[3]), __uint_as_float(x[4]), __uint_as_float(x[5])),
-                        fminf(__uint_as_float(x[6]), __uint_as_float(x[7])));
-        }
-        return fminf(fmin3(gm[0], gm[1], gm[2]), gm[3]);
-      } else {
-        // minimum: three-input tree of depth 4 (32 -> 11 -> 4 -> 1)
-        float m11[11];
-#pragma unroll
-        for (int j = 0; j < 10; j++)
-          m11[j] = fmin3(__uint_as_float(r[3 * j]), __uint_as_float(r[3 * j + 1]),
-                         __uint_as_float(r[3 * j + 2]));
-        m11[10] = fminf(__uint_as_float(r[30]), __uint_as_float(r[31]));
-        const float n0 = fmin3(m11[0], m11[1], m11[2]), n1 = fmin3(m11[3], m11[4], m11[5]);
-        const float n2 = fmin3(m11[6], m11[7], m11[8]), n3 = fminf(m11[9], m11[10]);
-        return fminf(fmin3(n0, n1, n2), n3);
-      }
+      for (int j = 0; j < 10; j++)
+        m11[j] = fmin3(__uint_as_float(r[3 * j]), __uint_as_float(r[3 * j + 1]),
+                       __uint_as_float(r[3 * j + 2]));
+      m11[10] = fminf(__uint_as_float(r[30]), __uint_as_float(r[31]));
+      const float n0 = fmin3(m11[0], m11[1], m11[2]), n1 = fmin3(m11[3], m11[4], m11[5]);
+      const float n2 = fmin3(m11[6], m11[7], m11[8]), n3 = fminf(m11[9], m11[10]);
+      return fminf(fmin3(n0, n1, n2), n3);
     };
     auto dbg_write = [&](const uint32_t (&r)[32], size_t cbase, int c0) {
       for (int i = 0; i < 32; i++) {
@@ -673,7 +658,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         for (int j = 0; j < w; j++) m16[j] = m16[2 * j] | m16[2 * j + 1];
       uint32_t mask = m16[0];
       s.n_sc++;
-      if constexpr (STG == 1) {
+      if constexpr (STG) {
 #pragma unroll
         for (int j = 0; j < 8; j++)
           reinterpret_cast<float4 *>(stage)[j ^ (lane & 7)] =
@@ -686,7 +671,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         const int i = (__ffs(mask) - 1) & 31;
         mask &= mask - 1;
         float vi;
-        if constexpr (STG == 1) {
+        if constexpr (STG) {
           vi = stage[((((i >> 2) ^ lane) & 7) << 2) | (i & 3)];  // the lane's own values
         } else {
           // v[i] for a runtime i: a 5-level select tree on the bits of i
@@ -703,41 +688,6 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                       pend, np);
         if (__any_sync(FULL_MASK, np == PEND)) {
           if (owner) epi_flush(s, heap, row, p.k, pend, np, ksh);
-        }
-      }
-    };
-    // Grouped slow part: a warp vote per 8-column group minimum, then per column of a flagged
-    // group, and the candidate step for the columns where some lane survives -- with
-    // compile-time register indices, so no pass mask and no runtime selection.
-    auto slow_grouped = [&](const uint32_t (&r)[32], const float (&gm)[4], size_t cbase,
-                            int c0) {
-      if (__any_sync(FULL_MASK, s.cnt > p.logcap - 32)) {
-        if (s.cnt > p.logcap - 32 && !s.ovf) {
-          s.cnt = log_compact(lg, s.cnt, s.thr);
-          if (s.cnt > p.logcap - 32) {
-            s.ovf = 1;
-            refresh_threshold(s);
-          }
-        }
-      }
-      s.n_sc++;
-      const uint32_t pos = (uint32_t)(cbase + c0);
-#pragma unroll
-      for (int g = 0; g < 4; g++) {
-        if (__any_sync(FULL_MASK, gm[g] <= s.Tv)) {
-#pragma unroll
-          for (int j = 8 * g; j < 8 * g + 8; j++) {
-            const float v = __uint_as_float(r[j]);
-            const bool act = v <= s.Tv;
-            if (__any_sync(FULL_MASK, act)) {
-              s.n_it++;
-              epi_candidate(s, v, pos + (uint32_t)j, act && valid, lg, p.logcap, owner, pend,
-                            np);
-              if (__any_sync(FULL_MASK, np == PEND)) {
-                if (owner) epi_flush(s, heap, row, p.k, pend, np, ksh);
-              }
-            }
-          }
         }
       }
     };
@@ -795,20 +745,14 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             __syncwarp();
             if (lane == 0) mbar_arrive(&tempty[b]);
           }
-          float ga[4], gb[4];
-          const float ma = fast(ra, cnt, c0, ga);
-          const float mb = fast(rb, cnt, c0 + 32, gb);
+          const float ma = fast(ra, cnt, c0);
+          const float mb = fast(rb, cnt, c0 + 32);
           if (p.dbg && valid) {
             dbg_write(ra, cbase, c0);
             dbg_write(rb, cbase, c0 + 32);
           }
-          if constexpr (STG == 2) {
-            if (__any_sync(FULL_MASK, ma <= s.Tv)) slow_grouped(ra, ga, cbase, c0);
-            if (__any_sync(FULL_MASK, mb <= s.Tv)) slow_grouped(rb, gb, cbase, c0 + 32);
-          } else {
-            if (__any_sync(FULL_MASK, ma <= s.Tv)) slow(ra, cbase, c0);
-            if (__any_sync(FULL_MASK, mb <= s.Tv)) slow(rb, cbase, c0 + 32);
-          }
+          if (__any_sync(FULL_MASK, ma <= s.Tv)) slow(ra, cbase, c0);
+          if (__any_sync(FULL_MASK, mb <= s.Tv)) slow(rb, cbase, c0 + 32);
         } else {
           uint32_t ra[32];
           __syncwarp();
@@ -820,14 +764,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             __syncwarp();
             if (lane == 0) mbar_arrive(&tempty[b]);
           }
-          float ga[4];
-          const float ma = fast(ra, cnt, c0, ga);
+          const float ma = fast(ra, cnt, c0);
           if (p.dbg && valid) dbg_write(ra, cbase, c0);
-          if constexpr (STG == 2) {
-            if (__any_sync(FULL_MASK, ma <= s.Tv)) slow_grouped(ra, ga, cbase, c0);
-          } else {
-            if (__any_sync(FULL_MASK, ma <= s.Tv)) slow(ra, cbase, c0);
-          }
+          if (__any_sync(FULL_MASK, ma <= s.Tv)) slow(ra, cbase, c0);
         }
       }
     }
@@ -1266,21 +1205,18 @@ static TcPlan tc_plan_base(int nq, int nc, int d, int k, int mode, int sms, bool
   // widest tile first, then the epilogue's shared-memory staging (with at least 2 stages), then
   // the deepest pipeline
   int best_N = 0, best_NST = 0, best_stg = 0;
-  // GSKNN_TC_STAGE=0/1/2 asks for a slow-path form (all give identical results); the plan
-  // falls back to form 0 where the asked one does not fit in shared memory
+  // GSKNN_TC_STAGE=0 keeps the staging areas out (both forms give identical results)
   static const char *stg_env = std::getenv("GSKNN_TC_STAGE");
-  static const int stg_want = stg_env ? std::max(0, std::min(2, std::atoi(stg_env))) : 1;
+  static const int stg_max = stg_env ? (std::atoi(stg_env) != 0) : 1;
   const int Ns[2] = {256, 128};
   for (int ni = 0; ni < 2 && !best_N; ni++) {
     const int N = Ns[ni];
     if (P.fmt == 0 && N == 256 && P.nkc > 4) continue;  // keep the TF32 A tile room
-    for (int stg : {stg_want, 0}) {
-      if (best_N) break;
+    for (int stg = stg_max; stg >= 0 && !best_N; stg--)
       for (int NST = 6; NST >= 2; NST--) {
         SmemLayout L = tc_smem_layout(P.nkc, P.a_terms, P.b_terms, N, NST, k, stg);
         if (L.total <= smem_max) { best_N = N; best_NST = NST; best_stg = stg; break; }
       }
-    }
   }
   if (!best_N) return P;
   P.N = best_N;
@@ -1470,12 +1406,9 @@ static cudaError_t tc_pass(const TcPlan &P, const TcCand &C, void *cand_pb, void
     if (r == cudaSuccess) kern<<<grid, NTHREADS, P.smem, st>>>(mA, mAlo, mB, mBlo, tp);
     return r;
   };
-  auto by_form = [&](auto k0, auto k1, auto k2) {
-    return P.stg == 2 ? launch(k2) : P.stg == 1 ? launch(k1) : launch(k0);
-  };
-  if (P.fmt == 0) e = by_form(tc_knn<0, 0>, tc_knn<0, 1>, tc_knn<0, 2>);
-  else if (P.fmt == 1) e = by_form(tc_knn<1, 0>, tc_knn<1, 1>, tc_knn<1, 2>);
-  else e = by_form(tc_knn<2, 0>, tc_knn<2, 1>, tc_knn<2, 2>);
+  if (P.fmt == 0) e = P.stg ? launch(tc_knn<0, true>) : launch(tc_knn<0, false>);
+  else if (P.fmt == 1) e = P.stg ? launch(tc_knn<1, true>) : launch(tc_knn<1, false>);
+  else e = P.stg ? launch(tc_knn<2, true>) : launch(tc_knn<2, false>);
   if (e == cudaSuccess) e = cudaGetLastError();
   mark(n_knn, false, 1);
   if (e != cudaSuccess) return e;
