@@ -32,8 +32,6 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
-#include <cstdlib>
-#include <type_traits>
 #include <cmath>
 
 namespace gsknn {
@@ -218,16 +216,11 @@ struct TcParams {
 };
 
 struct SmemLayout {
-  uint32_t a_off, b_off, heap_off, cn_off, stage_off, pend_off, bar_off, tmem_off, total;
+  uint32_t a_off, b_off, heap_off, cn_off, bar_off, tmem_off, total;
 };
 
-constexpr int PEND = 8;  // heap inserts a lane may defer before the warp flushes them
-
-// `stg`: the epilogue's staging areas are in shared memory too -- each epilogue warp's 32 x 32
-// chunk values (so the slow path reads a value at a runtime column with one load, not a select
-// tree) and its deferred-insert rings.
 __host__ __device__ inline SmemLayout tc_smem_layout(int nkc, int a_terms, int b_terms, int N,
-                                                     int NST, int k, int stg) {
+                                                     int NST, int k) {
   SmemLayout L;
   uint32_t off = 0;
   L.a_off = off;
@@ -239,14 +232,6 @@ __host__ __device__ inline SmemLayout tc_smem_layout(int nkc, int a_terms, int b
   off = (off + 15) & ~15u;
   L.cn_off = off;  // candidate norms of the tiles in flight, copied by the MMA warp
   off += (uint32_t)CN_SLOTS * N * 4;
-  off = (off + 15) & ~15u;
-  L.stage_off = off;
-  L.pend_off = off;
-  if (stg) {
-    off += (uint32_t)NEPI * 32 * 32 * 4;
-    L.pend_off = off;
-    off += (uint32_t)NEPI * PEND * 32 * 4;
-  }
   off = (off + 7) & ~7u;
   L.bar_off = off;
   off += (uint32_t)(2 * NST + 5 + CN_SLOTS) * 8;  // full, empty, tfull[2], tempty[2], afull, cnfull
@@ -316,44 +301,22 @@ __device__ __noinline__ int log_compact(uint2 *lg, int cnt, float thr) {
   return w;
 }
 
-// The deferred heap inserts of one lane: a register ring filled through compile-time indices
-// (so it stays in registers), or the lane's column of a per-warp ring in shared memory (one
-// store per insert instead of a predicated update of every register).
-struct RegRing {
-  float v[PEND];
-  __device__ __forceinline__ void init() {
-#pragma unroll
-    for (int j = 0; j < PEND; j++) v[j] = Num<float>::inf();
-  }
-  __device__ __forceinline__ void put(float dp, bool ins, int np) {
-#pragma unroll
-    for (int j = 0; j < PEND; j++) v[j] = (ins && j == np) ? dp : v[j];
-  }
-  __device__ __forceinline__ float get(int j) const { return v[j]; }
-};
-struct SmemRing {
-  float *p;  // [PEND][32] of this warp, lane-minor
-  int lane;
-  __device__ __forceinline__ void init() {}
-  __device__ __forceinline__ void put(float dp, bool ins, int np) {
-    if (ins) p[np * 32 + lane] = dp;
-  }
-  __device__ __forceinline__ float get(int j) const { return p[j * 32 + lane]; }
-};
+constexpr int PEND = 8;  // heap inserts a lane may defer before the warp flushes them
 
-template <class Ring>
-__device__ __forceinline__ void epi_defer(float dp, bool ins, Ring &pend, int &np) {
-  pend.put(dp, ins, np);
+// Defer the heap insert of `dp` (when `ins`) into a small register ring, filled through
+// compile-time indices so it stays in registers.
+__device__ __forceinline__ void epi_defer(float dp, bool ins, float (&pend)[PEND], int &np) {
+#pragma unroll
+  for (int j = 0; j < PEND; j++) pend[j] = (ins && j == np) ? dp : pend[j];
   np += ins ? 1 : 0;
 }
 
 // One candidate of the exact slow path: log it (when `act` and under the threshold) and, for
 // heap owners, defer its heap insert. Branch-free: every lane of the warp runs it, with
 // predicates instead of divergent branches.
-template <class Ring>
 __device__ __forceinline__ void epi_candidate(EpiState &s, float v, uint32_t id, bool act,
-                                              uint2 *lg, int logcap, bool owner, Ring &pend,
-                                              int &np) {
+                                              uint2 *lg, int logcap, bool owner,
+                                              float (&pend)[PEND], int &np) {
   const float dp = v + s.qn;
   const bool take = act && dp <= s.thr;
   s.n_ev += take ? 1u : 0u;
@@ -366,17 +329,13 @@ __device__ __forceinline__ void epi_candidate(EpiState &s, float v, uint32_t id,
 
 // Apply the deferred inserts (all lanes of the warp together, so their sift-downs overlap),
 // publish the new k-th to the other splits and tighten the threshold.
-template <class Ring>
-__device__ __forceinline__ void epi_flush(EpiState &s, float *heap, int row, int k, Ring &pend,
-                                          int &np, unsigned *ksh) {
+__device__ __forceinline__ void epi_flush(EpiState &s, float *heap, int row, int k,
+                                          float (&pend)[PEND], int &np, unsigned *ksh) {
 #pragma unroll
   for (int j = 0; j < PEND; j++) {
-    if (j < np) {
-      const float x = pend.get(j);
-      if (x < s.root) {
-        s.n_ins++;
-        s.root = heap_replace_root(heap, row, k, x);
-      }
+    if (j < np && pend[j] < s.root) {
+      s.n_ins++;
+      s.root = heap_replace_root(heap, row, k, pend[j]);
     }
   }
   np = 0;
@@ -388,7 +347,7 @@ __device__ __forceinline__ void epi_flush(EpiState &s, float *heap, int row, int
   refresh_threshold(s);
 }
 
-template <int FMT, bool STG>
+template <int FMT>
 __global__ void __launch_bounds__(NTHREADS, 1)
     tc_knn(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tAlo,
            const __grid_constant__ CUtensorMap tB, const __grid_constant__ CUtensorMap tBlo,
@@ -400,7 +359,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   if ((int)blockIdx.x * TC_M >= Qn) return;
   const uint32_t raw = su32(smem_raw);
   unsigned char *smem = smem_raw + ((1024u - (raw & 1023u)) & 1023u);
-  const SmemLayout L = tc_smem_layout(p.nkc, p.a_terms, p.b_terms, p.N, p.NST, p.k, STG);
+  const SmemLayout L = tc_smem_layout(p.nkc, p.a_terms, p.b_terms, p.N, p.NST, p.k);
   unsigned char *sA = smem + L.a_off;
   unsigned char *sB = smem + L.b_off;
   float *heap = reinterpret_cast<float *>(smem + L.heap_off);
@@ -549,16 +508,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     s.shared = Num<float>::inf();
     s.n_ev = s.n_ins = s.n_it = s.n_sc = 0;
     unsigned *ksh = p.kth_shared + (valid ? gq : 0);
-    using Ring = typename std::conditional<STG, SmemRing, RegRing>::type;
-    Ring pend;
-    if constexpr (STG) {
-      pend.p = reinterpret_cast<float *>(smem + L.pend_off) + (warp - 2) * PEND * 32;
-      pend.lane = lane;
-    }
-    pend.init();
+    float pend[PEND];
     int np = 0;
-    // this lane's 32 chunk values, swizzled by 16-byte slot so the stores do not conflict
-    float *stage = reinterpret_cast<float *>(smem + L.stage_off) + ((warp - 2) * 32 + lane) * 32;
+#pragma unroll
+    for (int j = 0; j < PEND; j++) pend[j] = Num<float>::inf();
     s.root = Num<float>::inf();
     s.qn = 0.0f;
     s.E2 = 0.0f;
@@ -658,33 +611,20 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         for (int j = 0; j < w; j++) m16[j] = m16[2 * j] | m16[2 * j + 1];
       uint32_t mask = m16[0];
       s.n_sc++;
-      if constexpr (STG) {
-#pragma unroll
-        for (int j = 0; j < 8; j++)
-          reinterpret_cast<float4 *>(stage)[j ^ (lane & 7)] =
-              make_float4(__uint_as_float(r[4 * j]), __uint_as_float(r[4 * j + 1]),
-                          __uint_as_float(r[4 * j + 2]), __uint_as_float(r[4 * j + 3]));
-      }
       while (__any_sync(FULL_MASK, mask != 0)) {
         s.n_it++;
         const bool act = mask != 0;
         const int i = (__ffs(mask) - 1) & 31;
         mask &= mask - 1;
-        float vi;
-        if constexpr (STG) {
-          vi = stage[((((i >> 2) ^ lane) & 7) << 2) | (i & 3)];  // the lane's own values
-        } else {
-          // v[i] for a runtime i: a 5-level select tree on the bits of i
-          float t16[16];
+        // v[i] for a runtime i: a 5-level select tree on the bits of i
+        float t16[16];
 #pragma unroll
-          for (int j = 0; j < 16; j++) t16[j] = __uint_as_float((i & 16) ? r[j + 16] : r[j]);
+        for (int j = 0; j < 16; j++) t16[j] = __uint_as_float((i & 16) ? r[j + 16] : r[j]);
 #pragma unroll
-          for (int w = 8, bit = 8; w >= 1; w >>= 1, bit >>= 1)
+        for (int w = 8, bit = 8; w >= 1; w >>= 1, bit >>= 1)
 #pragma unroll
-            for (int j = 0; j < w; j++) t16[j] = (i & bit) ? t16[j + w] : t16[j];
-          vi = t16[0];
-        }
-        epi_candidate(s, vi, (uint32_t)(cbase + c0 + i), act && valid, lg, p.logcap, owner,
+          for (int j = 0; j < w; j++) t16[j] = (i & bit) ? t16[j + w] : t16[j];
+        epi_candidate(s, t16[0], (uint32_t)(cbase + c0 + i), act && valid, lg, p.logcap, owner,
                       pend, np);
         if (__any_sync(FULL_MASK, np == PEND)) {
           if (owner) epi_flush(s, heap, row, p.k, pend, np, ksh);
@@ -1202,27 +1142,20 @@ static TcPlan tc_plan_base(int nq, int nc, int d, int k, int mode, int sms, bool
   if (k > 256) return P;
   // candidate tile width and pipeline depth that fit in shared memory
   const uint32_t smem_max = 227 * 1024;
-  // widest tile first, then the epilogue's shared-memory staging (with at least 2 stages), then
-  // the deepest pipeline
-  int best_N = 0, best_NST = 0, best_stg = 0;
-  // GSKNN_TC_STAGE=0 keeps the staging areas out (both forms give identical results)
-  static const char *stg_env = std::getenv("GSKNN_TC_STAGE");
-  static const int stg_max = stg_env ? (std::atoi(stg_env) != 0) : 1;
+  int best_N = 0, best_NST = 0;
   const int Ns[2] = {256, 128};
   for (int ni = 0; ni < 2 && !best_N; ni++) {
     const int N = Ns[ni];
     if (P.fmt == 0 && N == 256 && P.nkc > 4) continue;  // keep the TF32 A tile room
-    for (int stg = stg_max; stg >= 0 && !best_N; stg--)
-      for (int NST = 6; NST >= 2; NST--) {
-        SmemLayout L = tc_smem_layout(P.nkc, P.a_terms, P.b_terms, N, NST, k, stg);
-        if (L.total <= smem_max) { best_N = N; best_NST = NST; best_stg = stg; break; }
-      }
+    for (int NST = 6; NST >= 2; NST--) {
+      SmemLayout L = tc_smem_layout(P.nkc, P.a_terms, P.b_terms, N, NST, k);
+      if (L.total <= smem_max) { best_N = N; best_NST = NST; break; }
+    }
   }
   if (!best_N) return P;
   P.N = best_N;
   P.NST = best_NST;
-  P.stg = best_stg;
-  P.smem = tc_smem_layout(P.nkc, P.a_terms, P.b_terms, P.N, P.NST, k, P.stg).total;
+  P.smem = tc_smem_layout(P.nkc, P.a_terms, P.b_terms, P.N, P.NST, k).total;
   P.qtiles = (nq + TC_M - 1) / TC_M;
   P.r_pad = ((nc + 255) / 256) * 256;
   P.rtiles = P.r_pad / P.N;
@@ -1400,15 +1333,16 @@ static cudaError_t tc_pass(const TcPlan &P, const TcCand &C, void *cand_pb, void
   tp.rowmap = rowmap;
   dim3 grid(P.qtiles, P.S);
   mark(n_knn, true);
-  auto launch = [&](auto kern) {
-    cudaError_t r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         P.smem);
-    if (r == cudaSuccess) kern<<<grid, NTHREADS, P.smem, st>>>(mA, mAlo, mB, mBlo, tp);
-    return r;
-  };
-  if (P.fmt == 0) e = P.stg ? launch(tc_knn<0, true>) : launch(tc_knn<0, false>);
-  else if (P.fmt == 1) e = P.stg ? launch(tc_knn<1, true>) : launch(tc_knn<1, false>);
-  else e = P.stg ? launch(tc_knn<2, true>) : launch(tc_knn<2, false>);
+  if (P.fmt == 0) {
+    e = cudaFuncSetAttribute(tc_knn<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, P.smem);
+    if (e == cudaSuccess) tc_knn<0><<<grid, NTHREADS, P.smem, st>>>(mA, mAlo, mB, mBlo, tp);
+  } else if (P.fmt == 1) {
+    e = cudaFuncSetAttribute(tc_knn<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, P.smem);
+    if (e == cudaSuccess) tc_knn<1><<<grid, NTHREADS, P.smem, st>>>(mA, mAlo, mB, mBlo, tp);
+  } else {
+    e = cudaFuncSetAttribute(tc_knn<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, P.smem);
+    if (e == cudaSuccess) tc_knn<2><<<grid, NTHREADS, P.smem, st>>>(mA, mAlo, mB, mBlo, tp);
+  }
   if (e == cudaSuccess) e = cudaGetLastError();
   mark(n_knn, false, 1);
   if (e != cudaSuccess) return e;
