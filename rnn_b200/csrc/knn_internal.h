@@ -114,7 +114,6 @@ struct TcPlan {
   int fmt, elem, d_pad, nkc, a_terms, b_terms, kp;
   int N, NST, qtiles, rtiles, q_pad, r_pad, S, tiles_per_split, logcap;
   unsigned smem;
-  int two;  // built for two resident CTAs per SM (128-column tiles)
   float coefA, coefB;
   // query-side workspace offsets (absolute within the workspace; they start after the
   // prepared-candidate area when the plan includes it)

@@ -32,7 +32,6 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
-#include <cstdlib>
 #include <cmath>
 
 namespace gsknn {
@@ -220,11 +219,8 @@ struct SmemLayout {
   uint32_t a_off, b_off, heap_off, cn_off, bar_off, tmem_off, total;
 };
 
-// `two`: the form built for two resident CTAs per SM -- no staging of the candidate norms (the
-// epilogue reads them from global memory) and no alignment slack (the kernel checks that its
-// shared memory starts on a 1024-byte boundary).
 __host__ __device__ inline SmemLayout tc_smem_layout(int nkc, int a_terms, int b_terms, int N,
-                                                     int NST, int k, int two = 0) {
+                                                     int NST, int k) {
   SmemLayout L;
   uint32_t off = 0;
   L.a_off = off;
@@ -235,20 +231,15 @@ __host__ __device__ inline SmemLayout tc_smem_layout(int nkc, int a_terms, int b
   off += (uint32_t)k * TC_M * 4;
   off = (off + 15) & ~15u;
   L.cn_off = off;  // candidate norms of the tiles in flight, copied by the MMA warp
-  if (!two) off += (uint32_t)CN_SLOTS * N * 4;
+  off += (uint32_t)CN_SLOTS * N * 4;
   off = (off + 7) & ~7u;
   L.bar_off = off;
-  // full, empty, tfull[2], tempty[2], afull, cnfull
-  off += (uint32_t)(2 * NST + 5 + (two ? 0 : CN_SLOTS)) * 8;
+  off += (uint32_t)(2 * NST + 5 + CN_SLOTS) * 8;  // full, empty, tfull[2], tempty[2], afull, cnfull
   L.tmem_off = off;
   off += 16;
-  L.total = two ? off : off + 1024;  // alignment slack
+  L.total = off + 1024;  // alignment slack
   return L;
 }
-
-// Dynamic shared memory of one CTA when two are resident on an SM (228 KB per SM, 1 KB of it
-// reserved per CTA).
-constexpr uint32_t SMEM_TWO_MAX = (228u * 1024u) / 2u - 1024u;
 
 struct EpiState {
   float qn, E2, thr0, root, shared, thr, Tv;
@@ -356,11 +347,8 @@ __device__ __forceinline__ void epi_flush(EpiState &s, float *heap, int row, int
   refresh_threshold(s);
 }
 
-// TWO: the form for two resident CTAs per SM (register cap from the launch bounds, 32 accumulator
-// columns per TMEM wait, candidate norms read from global memory), which doubles the epilogue
-// warps per SM scheduler.
-template <int FMT, bool TWO>
-__global__ void __launch_bounds__(NTHREADS, TWO ? 2 : 1)
+template <int FMT>
+__global__ void __launch_bounds__(NTHREADS, 1)
     tc_knn(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tAlo,
            const __grid_constant__ CUtensorMap tB, const __grid_constant__ CUtensorMap tBlo,
            const TcParams p) {
@@ -370,14 +358,8 @@ __global__ void __launch_bounds__(NTHREADS, TWO ? 2 : 1)
   const int Qn = p.dQ ? *p.dQ : p.Q;
   if ((int)blockIdx.x * TC_M >= Qn) return;
   const uint32_t raw = su32(smem_raw);
-  if (TWO && (raw & 1023u) != 0u) {
-    // no slack to align the swizzled tiles: report instead (same for every thread of the CTA)
-    if (threadIdx.x == 0) atomicExch(p.status, GSKNN_ERR_UNSUPPORTED);
-    return;
-  }
   unsigned char *smem = smem_raw + ((1024u - (raw & 1023u)) & 1023u);
-  const SmemLayout L = tc_smem_layout(p.nkc, p.a_terms, p.b_terms, p.N, p.NST, p.k, TWO);
-  constexpr int STEP = TWO ? 32 : EPI_STEP;
+  const SmemLayout L = tc_smem_layout(p.nkc, p.a_terms, p.b_terms, p.N, p.NST, p.k);
   unsigned char *sA = smem + L.a_off;
   unsigned char *sB = smem + L.b_off;
   float *heap = reinterpret_cast<float *>(smem + L.heap_off);
@@ -410,8 +392,7 @@ __global__ void __launch_bounds__(NTHREADS, TWO ? 2 : 1)
       mbar_init(&tempty[b], NEPI);
     }
     mbar_init(afull, 1);
-    if (!TWO)
-      for (int c = 0; c < CN_SLOTS; c++) mbar_init(&cnfull[c], 1);
+    for (int c = 0; c < CN_SLOTS; c++) mbar_init(&cnfull[c], 1);
     mbar_fence_init();
   }
   if (warp == 1) {
@@ -471,12 +452,9 @@ __global__ void __launch_bounds__(NTHREADS, TWO ? 2 : 1)
         if (p.counters) w_tempty += clock64() - t0;
         // every epilogue warp has released tile lt - 2, so all of them are done with tile lt - 3
         // and its norm slot: fetch this tile's candidate norms there
-        if (!TWO) {
-          const int c = lt % CN_SLOTS;
-          mbar_expect_tx(&cnfull[c], (uint32_t)(N * 4));
-          bulk_g2s(cn_s + c * N, p.cn + (size_t)(t_begin + lt) * N, (uint32_t)(N * 4),
-                   &cnfull[c]);
-        }
+        const int c = lt % CN_SLOTS;
+        mbar_expect_tx(&cnfull[c], (uint32_t)(N * 4));
+        bulk_g2s(cn_s + c * N, p.cn + (size_t)(t_begin + lt) * N, (uint32_t)(N * 4), &cnfull[c]);
         tc_fence_after();
         const uint32_t tmem_d = tmem_base + (uint32_t)(b * N);
         for (int kc = 0; kc < p.nkc; kc++, it++) {
@@ -572,7 +550,7 @@ __global__ void __launch_bounds__(NTHREADS, TWO ? 2 : 1)
       const float4 *cn4 = reinterpret_cast<const float4 *>(cnt + c0);
 #pragma unroll
       for (int j = 0; j < 8; j++) {
-        const float4 c4 = TWO ? __ldg(cn4 + j) : cn4[j];
+        const float4 c4 = cn4[j];
         float v0, v1, v2, v3;
         fma2(v0, v1, __uint_as_float(r[4 * j + 0]), __uint_as_float(r[4 * j + 1]), -2.0f, c4.x,
              c4.y);
@@ -682,19 +660,19 @@ __global__ void __launch_bounds__(NTHREADS, TWO ? 2 : 1)
       }
       const long long t0 = p.counters ? clock64() : 0;
       if (!mbar_wait(&tfull[b], use & 1u)) { failed = true; break; }
-      if (!TWO && !mbar_wait(&cnfull[c], cuse & 1u)) { failed = true; break; }
+      if (!mbar_wait(&cnfull[c], cuse & 1u)) { failed = true; break; }
       if (p.counters) w_tfull += clock64() - t0;
       tc_fence_after();
       const uint32_t taddr = tmem_base + ((uint32_t)(lq * 32) << 16) + (uint32_t)(b * N);
+      const float *cnt = cn_s + c * N;
       const int tile = t_begin + lt;
-      const float *cnt = TWO ? p.cn + (size_t)tile * N : cn_s + c * N;
       const size_t cbase = (size_t)tile * N;
       // this warp's N/NPART columns, EPI_STEP at a time (one or two 32-column chunks per TMEM
       // wait); the accumulator is freed for the MMA warp once the tile's last loads of every
       // epilogue warp have landed (the norms stay in their own slot)
       const int cb = part * (N / NPART), ce = cb + N / NPART;
-      for (int c0 = cb; c0 < ce; c0 += STEP) {
-        if constexpr (STEP == 64) {
+      for (int c0 = cb; c0 < ce; c0 += EPI_STEP) {
+        if constexpr (EPI_STEP == 64) {
           uint32_t ra[32], rb[32];
           __syncwarp();
           tmem_ld32(taddr + (uint32_t)c0, ra);
@@ -1162,21 +1140,9 @@ static TcPlan tc_plan_base(int nq, int nc, int d, int k, int mode, int sms, bool
   P.kp = 32;
   while (P.kp < k) P.kp <<= 1;
   if (k > 256) return P;
-  // Two resident CTAs per SM (128-column tiles) where both fit in shared memory: twice the
-  // epilogue warps per SM scheduler. Otherwise one CTA per SM with the widest tile and the
-  // deepest pipeline that fit.
+  // candidate tile width and pipeline depth that fit in shared memory
   const uint32_t smem_max = 227 * 1024;
-  static const char *two_env = std::getenv("GSKNN_TC_TWO");  // 0: one CTA per SM only
-  const bool two_ok = !(two_env && std::atoi(two_env) == 0);
   int best_N = 0, best_NST = 0;
-  P.two = 0;
-  if (two_ok)
-    for (int NST = 4; NST >= 2 && !best_N; NST--)
-      if (tc_smem_layout(P.nkc, P.a_terms, P.b_terms, 128, NST, k, 1).total <= SMEM_TWO_MAX) {
-        best_N = 128;
-        best_NST = NST;
-        P.two = 1;
-      }
   const int Ns[2] = {256, 128};
   for (int ni = 0; ni < 2 && !best_N; ni++) {
     const int N = Ns[ni];
@@ -1189,7 +1155,7 @@ static TcPlan tc_plan_base(int nq, int nc, int d, int k, int mode, int sms, bool
   if (!best_N) return P;
   P.N = best_N;
   P.NST = best_NST;
-  P.smem = tc_smem_layout(P.nkc, P.a_terms, P.b_terms, P.N, P.NST, k, P.two).total;
+  P.smem = tc_smem_layout(P.nkc, P.a_terms, P.b_terms, P.N, P.NST, k).total;
   P.qtiles = (nq + TC_M - 1) / TC_M;
   P.r_pad = ((nc + 255) / 256) * 256;
   P.rtiles = P.r_pad / P.N;
@@ -1200,9 +1166,8 @@ static TcPlan tc_plan_base(int nq, int nc, int d, int k, int mode, int sms, bool
   double best = 1e300;
   for (int s = 1; s <= smax; s++) {
     const long long items = (long long)P.qtiles * s;
-    const int slots = sms * (P.two ? 2 : 1);
     // each split pays a start-up burst before the shared threshold tightens
-    const double cost = (double)((items + slots - 1) / slots) / s * (1.0 + 0.03 * s);
+    const double cost = (double)((items + sms - 1) / sms) / s * (1.0 + 0.03 * s);
     if (cost < best - 1e-12) { best = cost; best_s = s; }
   }
   P.S = best_s;
@@ -1368,15 +1333,16 @@ static cudaError_t tc_pass(const TcPlan &P, const TcCand &C, void *cand_pb, void
   tp.rowmap = rowmap;
   dim3 grid(P.qtiles, P.S);
   mark(n_knn, true);
-  auto launch = [&](auto kern) {
-    cudaError_t r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         P.smem);
-    if (r == cudaSuccess) kern<<<grid, NTHREADS, P.smem, st>>>(mA, mAlo, mB, mBlo, tp);
-    return r;
-  };
-  if (P.fmt == 0) e = P.two ? launch(tc_knn<0, true>) : launch(tc_knn<0, false>);
-  else if (P.fmt == 1) e = P.two ? launch(tc_knn<1, true>) : launch(tc_knn<1, false>);
-  else e = P.two ? launch(tc_knn<2, true>) : launch(tc_knn<2, false>);
+  if (P.fmt == 0) {
+    e = cudaFuncSetAttribute(tc_knn<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, P.smem);
+    if (e == cudaSuccess) tc_knn<0><<<grid, NTHREADS, P.smem, st>>>(mA, mAlo, mB, mBlo, tp);
+  } else if (P.fmt == 1) {
+    e = cudaFuncSetAttribute(tc_knn<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, P.smem);
+    if (e == cudaSuccess) tc_knn<1><<<grid, NTHREADS, P.smem, st>>>(mA, mAlo, mB, mBlo, tp);
+  } else {
+    e = cudaFuncSetAttribute(tc_knn<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, P.smem);
+    if (e == cudaSuccess) tc_knn<2><<<grid, NTHREADS, P.smem, st>>>(mA, mAlo, mB, mBlo, tp);
+  }
   if (e == cudaSuccess) e = cudaGetLastError();
   mark(n_knn, false, 1);
   if (e != cudaSuccess) return e;
