@@ -590,10 +590,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     // iteration (selected from its registers by index) and, for the row's owner, defers its
     // heap insert.
     auto slow = [&](const uint32_t (&r)[32], size_t cbase, int c0) {
+      // (a compaction that frees less than half of the log marks it overflowed: repeated
+      // compactions that each free a few entries would cost a full read of the log per chunk)
       if (__any_sync(FULL_MASK, s.cnt > p.logcap - 32)) {
         if (s.cnt > p.logcap - 32 && !s.ovf) {
           s.cnt = log_compact(lg, s.cnt, s.thr);
-          if (s.cnt > p.logcap - 32) {
+          if (s.cnt > p.logcap / 2) {
             s.ovf = 1;
             refresh_threshold(s);
           }
