@@ -110,7 +110,8 @@ __device__ __forceinline__ uint32_t to_tf32(float x) {
 // fmt: 0 = TF32 (4-byte panel), 1 = BF16, 2 = split BF16 (hi and lo panels)
 // Optional forms: `dcount` (device) replaces `count` and limits the panel to the tiles it needs;
 // `rowmap` packs point idx[rowmap[r]] as row r; `gate` (device) skips all work when it reads 0;
-// a null `enorm` writes the panels only (norms, bounds, ids and statistics are left alone).
+// a null `enorm` writes the panels only (norms, bounds, ids and statistics are left alone);
+// `pad_ok` packs index -1 as an empty padding row instead of reporting it.
 __global__ void __launch_bounds__(256) tc_pack(
     int fmt, const float *__restrict__ X, const float *__restrict__ X2, int d, int d_pad,
     long long nrows, const int *__restrict__ idx, int count, int rows_pad,
@@ -118,7 +119,7 @@ __global__ void __launch_bounds__(256) tc_pack(
     void *panel_lo, float *__restrict__ enorm, float *__restrict__ cnrm,
     uint32_t *__restrict__ ids, unsigned *__restrict__ stats, int *__restrict__ status,
     const int *__restrict__ dcount = nullptr, const int *__restrict__ rowmap = nullptr,
-    const int *__restrict__ gate = nullptr) {
+    const int *__restrict__ gate = nullptr, int pad_ok = 0) {
   const int lane = threadIdx.x & 31;
   const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (gate && *gate == 0) return;
@@ -131,7 +132,9 @@ __global__ void __launch_bounds__(256) tc_pack(
   long long row = -1;
   if (r < count) {
     row = idx[rowmap ? rowmap[r] : r];
-    if (row < 0 || row >= nrows) {
+    if (pad_ok && row == -1) {
+      // a padding row of a leaf panel (the batching form): silently empty
+    } else if (row < 0 || row >= nrows) {
       if (lane == 0) atomicExch(status, GSKNN_ERR_INDEX);
       row = -1;
     }
@@ -213,6 +216,13 @@ struct TcParams {
   // stride of the per-query arrays) and the heap row of each query
   const int *dQ;
   const int *rowmap;
+  // optional (batching form): one entry per CTA -- (query tile, first candidate tile, end
+  // candidate tile) -- in place of the (query tile, split) grid; rows whose rowmap entry is -1
+  // are padding
+  const int4 *qtab;
+  // a full log marks the query overflowed at once, without compacting it (a later pass in a
+  // narrower format finishes such queries)
+  int no_compact;
 };
 
 struct SmemLayout {
@@ -356,7 +366,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   // escalation pass: launched for the largest possible query count, the tiles past the count
   // on the device exit before any set-up
   const int Qn = p.dQ ? *p.dQ : p.Q;
-  if ((int)blockIdx.x * TC_M >= Qn) return;
+  if (!p.qtab && (int)blockIdx.x * TC_M >= Qn) return;
   const uint32_t raw = su32(smem_raw);
   unsigned char *smem = smem_raw + ((1024u - (raw & 1023u)) & 1023u);
   const SmemLayout L = tc_smem_layout(p.nkc, p.a_terms, p.b_terms, p.N, p.NST, p.k);
@@ -374,9 +384,17 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(smem + L.tmem_off);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int qt = blockIdx.x, split = blockIdx.y;
-  const int t_begin = split * p.tiles_per_split;
-  int t_end = t_begin + p.tiles_per_split;
+  int qt = blockIdx.x, t_begin, t_end;
+  const int split = blockIdx.y;
+  if (p.qtab) {
+    const int4 w = p.qtab[blockIdx.x];
+    qt = w.x;
+    t_begin = w.y;
+    t_end = w.z;
+  } else {
+    t_begin = split * p.tiles_per_split;
+    t_end = t_begin + p.tiles_per_split;
+  }
   if (t_end > p.ntiles_r) t_end = p.ntiles_r;
   const int ntile = t_end > t_begin ? t_end - t_begin : 0;
   const int N = p.N;
@@ -501,7 +519,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     const bool owner = part == 0;
     const int row = lq * 32 + lane;
     const int gq = qt * TC_M + row;
-    const bool valid = gq < Qn;
+    const bool valid = gq < Qn && (!p.rowmap || p.rowmap[gq] >= 0);
     EpiState s;
     s.cnt = 0;
     s.ovf = 0;
@@ -594,7 +612,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       // compactions that each free a few entries would cost a full read of the log per chunk)
       if (__any_sync(FULL_MASK, s.cnt > p.logcap - 32)) {
         if (s.cnt > p.logcap - 32 && !s.ovf) {
-          s.cnt = log_compact(lg, s.cnt, s.thr);
+          if (!p.no_compact) s.cnt = log_compact(lg, s.cnt, s.thr);
           if (s.cnt > p.logcap / 2) {
             s.ovf = 1;
             refresh_threshold(s);
@@ -673,6 +691,15 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       // wait); the accumulator is freed for the MMA warp once the tile's last loads of every
       // epilogue warp have landed (the norms stay in their own slot)
       const int cb = part * (N / NPART), ce = cb + N / NPART;
+      if (!p.dbg && __all_sync(FULL_MASK, !valid || s.ovf)) {
+        // every row of this warp is padding or finished by a later pass: release the
+        // accumulator without reading it (after its tile landed, so the release counts for
+        // this tile)
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&tempty[b]);
+        continue;
+      }
       for (int c0 = cb; c0 < ce; c0 += EPI_STEP) {
         if constexpr (EPI_STEP == 64) {
           uint32_t ra[32], rb[32];
@@ -756,7 +783,10 @@ struct RerankParams {
   int *fallback_count;
   unsigned long long *counters;  // optional: [5] entries scanned, [6] exact distances
   const int *dQ;      // optional: query count on the device (Q is then the stride)
-  const int *rowmap;  // optional: heap row (and query position in qidx) of each query
+  const int *rowmap;  // optional: heap row (and query position in qidx) of each query; -1: none
+  // batching form: candidates already in the incoming heap row (by id) are not entered twice,
+  // and overflowed queries go to the fallback list as their own positions q
+  int dedup;
 };
 
 // Exact squared distance of the oracle: (-2 <q,c> + |c|^2) + |q|^2 in FP64 from float inputs,
@@ -824,6 +854,16 @@ __device__ __forceinline__ void load_heap_row(const float *D, const int *I, int 
   warp_sort<double, E>(ld, li, lane);
 }
 
+// Whether `id` (NO_ID: never) is one of the ids the warp holds in `li` (E per lane).
+template <int E>
+__device__ __forceinline__ bool id_in_row(uint32_t id, const uint32_t (&li)[E]) {
+  bool hit = false;
+#pragma unroll
+  for (int e = 0; e < E; e++)
+    for (int src = 0; src < 32; src++) hit |= __shfl_sync(FULL_MASK, li[e], src) == id;
+  return hit && id != NO_ID;
+}
+
 template <int E>
 __global__ void __launch_bounds__(256) tc_rerank(RerankParams p) {
   __shared__ uint32_t rr_stage[8][64];
@@ -831,6 +871,7 @@ __global__ void __launch_bounds__(256) tc_rerank(RerankParams p) {
   const int q = blockIdx.x * 8 + (threadIdx.x >> 5);
   if (q >= (p.dQ ? *p.dQ : p.Q)) return;
   const int hr = p.rowmap ? p.rowmap[q] : q;  // heap row and query position
+  if (hr < 0) return;                          // a padding row of a leaf panel
   // overflowed logs: the query goes to the next pass (a narrower format, or brute force)
   bool ovf = false;
   float T = __uint_as_float(p.kth_shared[q]);  // NaN (all bits set) when nothing was published
@@ -839,7 +880,7 @@ __global__ void __launch_bounds__(256) tc_rerank(RerankParams p) {
     T = fminf(T, p.kth[(size_t)s * p.Q + q]);
   }
   if (ovf) {
-    if (lane == 0) p.fallback_list[atomicAdd(p.fallback_count, 1)] = hr;
+    if (lane == 0) p.fallback_list[atomicAdd(p.fallback_count, 1)] = p.dedup ? q : hr;
     return;
   }
   const float E2 = p.margin[q];
@@ -884,6 +925,9 @@ __global__ void __launch_bounds__(256) tc_rerank(RerankParams p) {
   double ld[E];
   uint32_t li[E];
   load_heap_row<E>(p.D, p.I, p.ldD, hr, p.k, ld, li, lane);
+  uint32_t li0[E];  // the incoming row's ids (the batching form's duplicate check)
+#pragma unroll
+  for (int e = 0; e < E; e++) li0[e] = li[e];
   const long long qrow = p.qidx[hr];
   const float *qv = p.Xq + qrow * p.d;
   const double qq = (double)p.Xq2[qrow];
@@ -898,6 +942,10 @@ __global__ void __launch_bounds__(256) tc_rerank(RerankParams p) {
     if (lane < count) {
       id = p.cid[stg[lane]];
       dist = exact_dist_lane(qv, p.Xc + (long long)id * p.d, p.d, (double)p.Xc2[id], qq);
+    }
+    if (p.dedup && id_in_row<E>(id, li0)) {
+      dist = Num<double>::inf();
+      id = NO_ID;
     }
     if (p.counters && lane == 0) atomicAdd(&p.counters[6], (unsigned long long)count);
     double b1[1] = {dist};
@@ -1018,6 +1066,62 @@ __global__ void __launch_bounds__(256) tc_fallback(FallbackParams p) {
       write_heap_row<E>(p.D, p.I, p.ldD, q, p.k, md, mi, lane);
     }
     __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// batching form: exact brute force of overflowed queries over their own leaf
+// ------------------------------------------------------------------------------------------
+struct LeafFallbackParams {
+  int k, d, N;                 // N: candidate tile width of the panel
+  const float *X, *X2;         // the point table
+  const int *rowmap;           // panel row -> point (heap row)
+  const uint32_t *ids;         // panel row -> point id (NO_ID: padding)
+  const int2 *rtab;            // panel query tile -> (first, end) candidate tile of its leaf
+  float *D;
+  int *I;
+  int ldD;
+  const int *list;             // panel rows
+  const int *count;
+};
+
+// One warp per listed query: the exact FP64 distances to every point of its leaf, merged with
+// the incoming heap row (ids already there are not entered twice).
+template <int E>
+__global__ void __launch_bounds__(256) tc_fallback_leaf(LeafFallbackParams p) {
+  const int lane = threadIdx.x & 31;
+  const int n = *p.count;
+  for (int w = blockIdx.x * 8 + (threadIdx.x >> 5); w < n; w += gridDim.x * 8) {
+    const int q = p.list[w];
+    const int hr = p.rowmap[q];
+    const int2 r = p.rtab[q / TC_M];
+    const float *qv = p.X + (long long)hr * p.d;
+    const double qq = (double)p.X2[hr];
+    double ld[E];
+    uint32_t li[E];
+    load_heap_row<E>(p.D, p.I, p.ldD, hr, p.k, ld, li, lane);
+    uint32_t li0[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) li0[e] = li[e];
+    for (int base = r.x * p.N; base < r.y * p.N; base += 32) {  // warp-uniform trip count
+      const int c = base + lane;
+      uint32_t id = NO_ID;
+      double dist = Num<double>::inf();
+      if (c < r.y * p.N) {
+        id = p.ids[c];
+        if (id != NO_ID)
+          dist = exact_dist_lane(qv, p.X + (long long)id * p.d, p.d, (double)p.X2[id], qq);
+      }
+      if (id_in_row<E>(id, li0)) {
+        dist = Num<double>::inf();
+        id = NO_ID;
+      }
+      double b1[1] = {dist};
+      uint32_t i1[1] = {id};
+      warp_sort<double, 1>(b1, i1, lane);
+      warp_merge_32<double, E>(ld, li, b1[0], i1[0], lane);
+    }
+    write_heap_row<E>(p.D, p.I, p.ldD, hr, p.k, ld, li, lane);
   }
 }
 
@@ -1333,6 +1437,7 @@ static cudaError_t tc_pass(const TcPlan &P, const TcCand &C, void *cand_pb, void
   tp.counters = counters;
   tp.dQ = dQ;
   tp.rowmap = rowmap;
+  tp.no_compact = P.esc_mode != 0;
   dim3 grid(P.qtiles, P.S);
   mark(n_knn, true);
   if (P.fmt == 0) {
