@@ -275,9 +275,14 @@ void gsknn_release_workspace(void);
  * One pass is one persistent launch over all leaves (work items dealt by an atomic counter,
  * longest first), packed and merged by two more kernels, captured once in a CUDA graph and
  * replayed for every pass on `stream`. `leaf_min` bounds the smallest leaf (it sizes the
- * buffers); `shape` picks the tile shape (0: 128-row tiles, 1 and 2: 64-row tiles) or, with
- * -1, lets the autotuner time every shape on the first pass of each (d, k, mean leaf size)
- * class and remember the fastest for the process. Passes are asynchronous: gsknn_batch_pass
+ * buffers); `shape` picks the tile shape (0: 128-row tiles, 1 and 2: 64-row tiles on the CUDA
+ * cores; 3: the tensor-core shape) or, with -1, lets the autotuner time every shape on the
+ * first pass of each (d, k, mean leaf size) class and remember the fastest for the process.
+ * The tensor-core shape runs the precision form per tree: the tree's leaves laid out in one
+ * split-BF16 panel (each leaf padded to whole 256-point tiles), every query tile against its own
+ * leaf's tiles, and the exact FP64 re-rank merging straight into the heap rows, entering no id
+ * twice; its results are the exact FP64 neighbours (the CUDA-core shapes give FP32 ones). It is
+ * not open to jobs whose rows stand for global ids (the streaming form). Passes are asynchronous: gsknn_batch_pass
  * returns once the pass is enqueued (it waits only for the previous pass's plan upload);
  * gsknn_batch_sync waits and reports index errors. */
 typedef struct gsknn_batch_s gsknn_batch_t;
@@ -288,8 +293,8 @@ int gsknn_batch_pass(gsknn_batch_t *job, const int *leaf_ptr, const int *leaf_pt
                      const int *leaf_tree, int nleaves);
 int gsknn_batch_sync(gsknn_batch_t *job);
 /* Shape in use, its tile rows, persistent grid, tiles / work items / distance evaluations of
- * the last pass, and (when this job ran the autotuner) the trial time of each shape in ms
- * (-1: not tried). Any pointer may be NULL. */
+ * the last pass, and (when this job ran the autotuner) the trial time of each of the 4 shapes
+ * in ms (-1: not tried; tune_ms holds 4 entries). Any pointer may be NULL. */
 int gsknn_batch_info(const gsknn_batch_t *job, int *shape, int *tile_rows, int *grid,
                      int *tiles, int *items, double *evals, float *tune_ms);
 void gsknn_batch_destroy(gsknn_batch_t *job);

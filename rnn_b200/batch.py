@@ -16,7 +16,7 @@ import numpy as np
 from rnn_b200 import gsknn as G
 
 SHAPES = {0: "128-row tiles, 8x8 per thread", 1: "64-row tiles, 8x4 per thread",
-          2: "64-row tiles, 4x4 per thread"}
+          2: "64-row tiles, 4x4 per thread", 3: "tensor cores, split BF16 + FP64 re-rank"}
 
 
 @dataclass
@@ -134,14 +134,14 @@ class BatchJob:
         ci = ctypes.c_int
         shape, rows, grid, tiles, items = ci(), ci(), ci(), ci(), ci()
         evals = ctypes.c_double()
-        tune = (ctypes.c_float * 3)()
+        tune = (ctypes.c_float * 4)()
         self._L.gsknn_batch_info(self._h, ctypes.byref(shape), ctypes.byref(rows),
                                  ctypes.byref(grid), ctypes.byref(tiles), ctypes.byref(items),
                                  ctypes.byref(evals), tune)
         return {"shape": shape.value, "shape_name": SHAPES.get(shape.value, "?"),
                 "tile_rows": rows.value, "grid": grid.value, "tiles": tiles.value,
                 "items": items.value, "evals": evals.value,
-                "tune_ms": {SHAPES[s]: round(float(tune[s]), 3) for s in range(3)
+                "tune_ms": {SHAPES[s]: round(float(tune[s]), 3) for s in range(4)
                             if tune[s] >= 0}}
 
     def close(self) -> None:

@@ -44,7 +44,8 @@ template <int KP, int SHAPE> struct Shape;
 template <int KP> struct Shape<KP, 0> { using C = SimtCfg<float, KP, 2, 2, 4, 2, DK, 3>; };
 template <int KP> struct Shape<KP, 1> { using C = SimtCfg<float, KP, 2, 1, 2, 2, DK, 3>; };
 template <int KP> struct Shape<KP, 2> { using C = SimtCfg<float, KP, 1, 1, 4, 2, DK, 3>; };
-constexpr int NSHAPES = 3;
+constexpr int NSHAPES = 3;   // CUDA-core tile shapes
+constexpr int SHAPE_TC = 3;  // the tensor-core shape (split BF16 + FP64 re-rank per tree)
 inline int shape_bt(int shape) { return shape == 0 ? 128 : 64; }
 inline bool shape_ok(int shape, int kp) { return kp <= 64 || shape != 0; }
 
@@ -322,7 +323,7 @@ static cudaError_t launch_merge(int kp, float *D, int *I, int ldD, int N, int k,
 
 // process-wide autotuner memory: (d, kp, mean leaf size rounded to a power of two) -> shape
 static std::mutex g_tune_mu;
-static std::map<std::tuple<int, int, int>, int> g_tuned;
+static std::map<std::tuple<int, int, int, int>, int> g_tuned;
 
 static int size_class(double mean_leaf) {
   int c = 1;
@@ -372,6 +373,22 @@ struct BatchJob {
   // last pass
   int last_tiles, last_items;
   double last_evals;
+  // tensor-core shape: one leaf panel per tree, the trees run one after another, each query
+  // tile against its own leaf's candidate tiles, the exact re-rank merging into the heap
+  int tc_tile;                  // candidate tile width of the panels (0: not available)
+  TcLeafPlan tcl;               // plan of the allocated workspace (tcl.ok: allocated)
+  void *tc_ws;
+  int *tc_pidx;                 // device: every tree's panel rows (point or -1)
+  int4 *tc_qtab;                // device: every tree's query-tile table
+  int2 *tc_rtab;                // device: candidate tile range of every panel query tile
+  int *h_tc_pidx;               // pinned staging of the three
+  int4 *h_tc_qtab;
+  int2 *h_tc_rtab;
+  long long tc_cap_rows;        // capacity (rows over all trees) of the arrays above
+  long long *h_tc_tree;         // per tree: rows, query tiles, and the offsets of the three
+  float *tD;                    // scratch heap for timing the tensor-core shape
+  int *tI;
+  float tune_tc_ms;
 };
 
 }  // namespace gsknn
@@ -470,6 +487,154 @@ static cudaError_t upload_plan(BatchJob *b, int BT, int ntiles, int nitems) {
   return e;
 }
 
+// ---- tensor-core shape -----------------------------------------------------------------------
+// Per tree of the pass: its leaves laid out at multiples of the tile width, the query tiles that
+// hold real rows (each with its leaf's candidate tile range) and, for every panel query tile,
+// the range (the leaf brute force's lookup). Fills the pinned staging and the per-tree table.
+static int build_tc_plan(BatchJob *b, const int *leaf_ptr, const int *leaf_pts,
+                         const int *leaf_tree, int nleaves, double *evals, long long *need_rows,
+                         int *max_tree_rows) {
+  const int NT = b->tc_tile;
+  std::vector<long long> rows(b->T, 0), nq(b->T, 0);
+  double ev = 0.0;
+  for (int l = 0; l < nleaves; l++) {
+    const int L = leaf_ptr[l + 1] - leaf_ptr[l];
+    if (L < 0) return set_err(GSKNN_ERR_ARG, "leaf_ptr must be non-decreasing");
+    const int t = leaf_tree[l];
+    if (t < 0 || t >= b->T)
+      return set_err(GSKNN_ERR_ARG, "leaf_tree entries must lie in [0, trees_per_pass)");
+    if (L == 0) continue;
+    rows[t] += (long long)(L + NT - 1) / NT * NT;
+    nq[t] += (L + 127) / 128;
+    ev += (double)L * L;
+  }
+  long long tot = 0, mx = 0;
+  for (int t = 0; t < b->T; t++) {
+    tot += rows[t];
+    mx = std::max(mx, rows[t]);
+  }
+  *need_rows = tot;
+  *max_tree_rows = (int)std::min<long long>(mx, 1LL << 30);
+  *evals = ev;
+  if (tot > b->tc_cap_rows) return GSKNN_OK;  // the caller grows the arrays and calls again
+  long long po = 0, qo = 0;
+  for (int t = 0; t < b->T; t++) {
+    long long *tr = b->h_tc_tree + 6 * t;
+    tr[0] = rows[t];
+    tr[1] = 0;
+    tr[2] = po;       // panel rows offset
+    tr[3] = qo;       // query-tile table offset
+    tr[4] = po / 128; // range table offset
+    tr[5] = 0;        // rows laid out so far
+    po += rows[t];
+    qo += nq[t];
+  }
+  for (int l = 0; l < nleaves; l++) {
+    const int L = leaf_ptr[l + 1] - leaf_ptr[l];
+    if (L == 0) continue;
+    long long *tr = b->h_tc_tree + 6 * leaf_tree[l];
+    const long long r0 = tr[5];
+    const int span = (L + NT - 1) / NT * NT;
+    int *dst = b->h_tc_pidx + tr[2] + r0;
+    for (int r = 0; r < span; r++) dst[r] = r < L ? leaf_pts[leaf_ptr[l] + r] : -1;
+    const int tb = (int)(r0 / NT), te = tb + span / NT;
+    for (long long q = r0 / 128; q * 128 < r0 + L; q++)
+      b->h_tc_qtab[tr[3] + tr[1]++] = make_int4((int)q, tb, te, 0);
+    for (long long q = r0 / 128; q * 128 < r0 + span; q++)
+      b->h_tc_rtab[tr[4] + q] = make_int2(tb, te);
+    tr[5] += span;
+  }
+  return GSKNN_OK;
+}
+
+static void free_tc(BatchJob *b) {
+  if (b->tc_ws) cudaFree(b->tc_ws);
+  if (b->tc_pidx) cudaFree(b->tc_pidx);
+  if (b->h_tc_pidx) cudaFreeHost(b->h_tc_pidx);
+  if (b->h_tc_qtab) cudaFreeHost(b->h_tc_qtab);
+  if (b->h_tc_rtab) cudaFreeHost(b->h_tc_rtab);
+  b->tc_ws = nullptr;
+  b->tc_pidx = nullptr;
+  b->h_tc_pidx = nullptr;
+  b->h_tc_qtab = nullptr;
+  b->h_tc_rtab = nullptr;
+  b->tc_cap_rows = 0;
+  b->tcl.ok = false;
+}
+
+// Workspace and plan arrays for `rows` panel rows over all trees, `tree_rows` for one tree (with
+// a margin, so that later passes rarely need to grow them).
+static int ensure_tc(BatchJob *b, long long rows, int tree_rows) {
+  if (b->tcl.ok && rows <= b->tc_cap_rows && tree_rows <= b->tcl.rows_cap) return GSKNN_OK;
+  BCU(cudaStreamSynchronize(b->st));
+  BCU(cudaEventSynchronize(b->staged));
+  free_tc(b);
+  const long long cap = (rows + rows / 8 + 128 * b->T + 127) / 128 * 128;
+  const long long tcap = ((long long)tree_rows + tree_rows / 8 + 127) / 128 * 128;
+  b->tcl = gsknn::tc_leaf_plan(b->N, (int)std::min<long long>(tcap, 1LL << 30), b->d, b->k,
+                               b->sms);
+  if (!b->tcl.ok) return set_err(GSKNN_ERR_UNSUPPORTED, "tensor-core shape: no tile plan");
+  const size_t pb = (size_t)cap * 4, qb = (size_t)(cap / 128) * sizeof(int4),
+               rb = (size_t)(cap / 128) * sizeof(int2);
+  if (cudaMalloc(&b->tc_ws, b->tcl.bytes) != cudaSuccess ||
+      cudaMalloc((void **)&b->tc_pidx, pb + qb + rb + 512) != cudaSuccess ||
+      cudaHostAlloc((void **)&b->h_tc_pidx, pb, cudaHostAllocDefault) != cudaSuccess ||
+      cudaHostAlloc((void **)&b->h_tc_qtab, qb, cudaHostAllocDefault) != cudaSuccess ||
+      cudaHostAlloc((void **)&b->h_tc_rtab, rb, cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    free_tc(b);
+    return set_err(GSKNN_ERR_NOMEM, "tensor-core shape: device memory exhausted");
+  }
+  char *base = reinterpret_cast<char *>(b->tc_pidx);
+  b->tc_qtab = reinterpret_cast<int4 *>(base + ((pb + 255) & ~(size_t)255));
+  b->tc_rtab = reinterpret_cast<int2 *>(base + ((pb + 255) & ~(size_t)255) +
+                                        ((qb + 255) & ~(size_t)255));
+  b->tc_cap_rows = cap;
+  return GSKNN_OK;
+}
+
+// Upload the staged tensor-core plan and enqueue every tree's pass on the heap D / I.
+static int enqueue_tc_pass(BatchJob *b, float *D, int *I) {
+  long long prow = 0, pq = 0;
+  for (int t = 0; t < b->T; t++) {
+    prow += b->h_tc_tree[6 * t];
+    pq += b->h_tc_tree[6 * t + 1];
+  }
+  BCU(cudaMemcpyAsync(b->tc_pidx, b->h_tc_pidx, (size_t)prow * 4, cudaMemcpyHostToDevice,
+                      b->st));
+  BCU(cudaMemcpyAsync(b->tc_qtab, b->h_tc_qtab, (size_t)pq * sizeof(int4),
+                      cudaMemcpyHostToDevice, b->st));
+  BCU(cudaMemcpyAsync(b->tc_rtab, b->h_tc_rtab, (size_t)(prow / 128) * sizeof(int2),
+                      cudaMemcpyHostToDevice, b->st));
+  BCU(cudaEventRecord(b->staged, b->st));
+  for (int t = 0; t < b->T; t++) {
+    const long long *tr = b->h_tc_tree + 6 * t;
+    if (tr[1] == 0) continue;
+    BCU(gsknn::tc_leaf_pass(b->tcl, b->tc_ws, b->X, b->X2, b->N, b->d, b->k,
+                            b->tc_pidx + tr[2], (int)tr[0], b->tc_qtab + tr[3], (int)tr[1],
+                            b->tc_rtab + tr[4], D, I, b->ldD, b->status, b->st));
+  }
+  return GSKNN_OK;
+}
+
+// Plan, grow and enqueue one tensor-core pass.
+static int tc_pass(BatchJob *b, const int *leaf_ptr, const int *leaf_pts, const int *leaf_tree,
+                   int nleaves, float *D, int *I, double *evals) {
+  if (b->gid) return set_err(GSKNN_ERR_UNSUPPORTED, "tensor-core shape: not for global ids");
+  BCU(cudaEventSynchronize(b->staged));  // the staging of the previous upload is free
+  long long need = 0;
+  int tmax = 0;
+  int rc = build_tc_plan(b, leaf_ptr, leaf_pts, leaf_tree, nleaves, evals, &need, &tmax);
+  if (rc != GSKNN_OK) return rc;
+  if (!b->tcl.ok || need > b->tc_cap_rows || tmax > b->tcl.rows_cap) {
+    rc = ensure_tc(b, need, tmax);
+    if (rc != GSKNN_OK) return rc;
+    rc = build_tc_plan(b, leaf_ptr, leaf_pts, leaf_tree, nleaves, evals, &need, &tmax);
+    if (rc != GSKNN_OK) return rc;
+  }
+  return enqueue_tc_pass(b, D, I);
+}
+
 namespace gsknn {
 // Rows of the job's table stand for the global points gid[row] (device array, N entries): the
 // lists and the heap carry those ids, while leaves, stamps and heap rows index the table.
@@ -492,7 +657,7 @@ gsknn_batch_t *gsknn_batch_create(int N, int d, int k, const float *X, const flo
     set_err(GSKNN_ERR_UNSUPPORTED, "gsknn_batch_create: k > 256 is not supported");
     return nullptr;
   }
-  if (shape >= gb::NSHAPES) {
+  if (shape > gb::SHAPE_TC) {
     set_err(GSKNN_ERR_ARG, "gsknn_batch_create: unknown tile shape");
     return nullptr;
   }
@@ -501,7 +666,7 @@ gsknn_batch_t *gsknn_batch_create(int N, int d, int k, const float *X, const flo
   b->N = N; b->d = d; b->k = k; b->ldD = ldD; b->T = trees_per_pass; b->leaf_min = leaf_min;
   b->kp = 32;
   while (b->kp < k) b->kp <<= 1;
-  if (shape >= 0 && !gb::shape_ok(shape, b->kp)) {
+  if (shape >= 0 && shape < gb::NSHAPES && !gb::shape_ok(shape, b->kp)) {
     delete b;
     set_err(GSKNN_ERR_UNSUPPORTED, "gsknn_batch_create: 128-row tiles need k <= 64");
     return nullptr;
@@ -513,6 +678,14 @@ gsknn_batch_t *gsknn_batch_create(int N, int d, int k, const float *X, const flo
   int dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
+  b->tc_tile = gsknn::tc_leaf_tile(d, k, b->sms);
+  b->tune_tc_ms = -1.f;
+  if (shape == gb::SHAPE_TC && b->tc_tile == 0) {
+    delete b;
+    set_err(GSKNN_ERR_UNSUPPORTED, "gsknn_batch_create: no tensor-core tile plan for d and k");
+    return nullptr;
+  }
+  b->h_tc_tree = new long long[6 * (size_t)trees_per_pass]();
   // every leaf pads to whole tiles: at most 127 rows each at 128-row tiles
   const long long leaves = (long long)trees_per_pass * ((N + leaf_min - 1) / leaf_min);
   const long long max_rows = (long long)trees_per_pass * N + 128 * leaves;
@@ -593,7 +766,8 @@ int gsknn_batch_pass(gsknn_batch_t *job, const int *leaf_ptr, const int *leaf_pt
   BCU(cudaStreamWaitEvent(b->st, b->ev_in, 0));
   // tune on this pass's leaves if no shape is known for (d, k, leaf size)
   const double mean_leaf = (double)(leaf_ptr[nleaves] - leaf_ptr[0]) / nleaves;
-  const auto key = std::make_tuple(b->d, b->kp, gb::size_class(mean_leaf));
+  // (the tensor-core shape is not open to jobs with global ids, so they tune apart)
+  const auto key = std::make_tuple(b->d, b->kp, gb::size_class(mean_leaf), b->gid ? 1 : 0);
   if (b->shape < 0) {
     std::lock_guard<std::mutex> lk(gb::g_tune_mu);
     auto it = gb::g_tuned.find(key);
@@ -606,6 +780,33 @@ int gsknn_batch_pass(gsknn_batch_t *job, const int *leaf_ptr, const int *leaf_pt
     BCU(cudaEventCreate(&e1));
     float best = 0.f;
     int best_s = -1;
+    // the tensor-core shape writes the heap as it goes: it is timed on a scratch copy
+    b->tune_tc_ms = -1.f;
+    if (b->tc_tile > 0 && !b->gid) {
+      const size_t hb = (size_t)b->N * b->ldD * 4;
+      if (!b->tD) {
+        if (cudaMalloc((void **)&b->tD, hb) != cudaSuccess ||
+            cudaMalloc((void **)&b->tI, hb) != cudaSuccess) {
+          cudaGetLastError();
+          return set_err(GSKNN_ERR_NOMEM, "gsknn_batch_pass: no memory to tune");
+        }
+      }
+      double ev = 0;
+      for (int rep = 0; rep < 2; rep++) {  // warm-up (workspace, modules), then timed
+        BCU(cudaMemcpyAsync(b->tD, b->D, hb, cudaMemcpyDeviceToDevice, b->st));
+        BCU(cudaMemcpyAsync(b->tI, b->I, hb, cudaMemcpyDeviceToDevice, b->st));
+        BCU(cudaEventRecord(e0, b->st));
+        const int rc = tc_pass(b, leaf_ptr, leaf_pts, leaf_tree, nleaves, b->tD, b->tI, &ev);
+        if (rc != GSKNN_OK) return rc;
+        BCU(cudaEventRecord(e1, b->st));
+        BCU(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        BCU(cudaEventElapsedTime(&ms, e0, e1));
+        b->tune_tc_ms = ms;
+      }
+      best = b->tune_tc_ms;
+      best_s = gb::SHAPE_TC;
+    }
     for (int s = 0; s < gb::NSHAPES; s++) {
       b->tune_ms[s] = -1.f;
       if (!gb::shape_ok(s, b->kp)) continue;
@@ -636,6 +837,23 @@ int gsknn_batch_pass(gsknn_batch_t *job, const int *leaf_ptr, const int *leaf_pt
     b->tuned_here = true;
     std::lock_guard<std::mutex> lk(gb::g_tune_mu);
     gb::g_tuned[key] = best_s;
+  }
+  if (b->shape == gb::SHAPE_TC) {
+    double ev = 0;
+    const int rc = tc_pass(b, leaf_ptr, leaf_pts, leaf_tree, nleaves, b->D, b->I, &ev);
+    if (rc != GSKNN_OK) return rc;
+    BCU(cudaEventRecord(b->ev_out, b->st));
+    BCU(cudaStreamWaitEvent(b->user, b->ev_out, 0));
+    long long q = 0, rows = 0;
+    for (int t = 0; t < b->T; t++) {
+      rows += b->h_tc_tree[6 * t];
+      q += b->h_tc_tree[6 * t + 1];
+    }
+    b->last_tiles = (int)(rows / 128);
+    b->last_items = (int)q;
+    b->last_evals = ev;
+    gsknn::set_status(GSKNN_OK, nullptr);
+    return GSKNN_OK;
   }
   const int BT = gb::shape_bt(b->shape);
   int tiles = 0, items = 0;
@@ -689,14 +907,17 @@ int gsknn_batch_info(const gsknn_batch_t *job, int *shape, int *tile_rows, int *
                      int *tiles, int *items, double *evals, float *tune_ms) {
   const BatchJob *b = reinterpret_cast<const BatchJob *>(job);
   if (!b) return set_err(GSKNN_ERR_ARG, "gsknn_batch_info: null job");
+  const bool tc = b->shape == gb::SHAPE_TC;
   if (shape) *shape = b->shape;
-  if (tile_rows) *tile_rows = b->shape >= 0 ? gb::shape_bt(b->shape) : 0;
-  if (grid) *grid = b->shape >= 0 ? b->grid[b->shape] : 0;
+  if (tile_rows) *tile_rows = tc ? b->tc_tile : b->shape >= 0 ? gb::shape_bt(b->shape) : 0;
+  if (grid) *grid = tc ? b->last_items : b->shape >= 0 ? b->grid[b->shape] : 0;
   if (tiles) *tiles = b->last_tiles;
   if (items) *items = b->last_items;
   if (evals) *evals = b->last_evals;
-  if (tune_ms)
+  if (tune_ms) {
     for (int s = 0; s < gb::NSHAPES; s++) tune_ms[s] = b->tuned_here ? b->tune_ms[s] : -1.f;
+    tune_ms[gb::SHAPE_TC] = b->tuned_here ? b->tune_tc_ms : -1.f;
+  }
   return GSKNN_OK;
 }
 
@@ -714,6 +935,10 @@ void gsknn_batch_destroy(gsknn_batch_t *job) {
   if (b->h_items) cudaFreeHost(b->h_items);
   if (b->h_meta) cudaFreeHost(b->h_meta);
   if (b->dbuf) cudaFree(b->dbuf);
+  free_tc(b);
+  if (b->tD) cudaFree(b->tD);
+  if (b->tI) cudaFree(b->tI);
+  delete[] b->h_tc_tree;
   delete b;
 }
 

@@ -177,6 +177,26 @@ cudaError_t tc_run(const TcPlan &P, int nq, int nc, int d, int k, const float *X
                    int ldD, void *ws, int *status, float *dbg, long long dbg_ld,
                    unsigned long long *counters, cudaStream_t st, TraceHook hook,
                    void *hook_ctx);
+// Tensor-core form of the batching pass (all-NN within randomized-tree leaves): one tree's
+// leaves laid out in a panel, each leaf padded to whole candidate tiles; every query tile runs
+// against its own leaf's tiles only, and the exact re-rank merges into the heap rows in place,
+// entering no id twice (a point reached again by another tree or pass).
+struct TcLeafPlan {
+  bool ok;
+  TcPlan P;        // the split-BF16 tile plan (one split), per-query area for rows_cap rows
+  int rows_cap;    // panel rows one tree may need
+  size_t o_mu, o_mu2, o_stats, o_pb, o_pb_lo, o_cn, o_cnrm, o_cid, o_iota, bytes;
+};
+// npts: points of the table; rows_cap: panel rows one tree may use (a multiple of 128).
+TcLeafPlan tc_leaf_plan(long long npts, int rows_cap, int d, int k, int sms);
+// Candidate tile width of the leaf panels: every leaf starts at a multiple of it (0: no plan).
+int tc_leaf_tile(int d, int k, int sms);
+// One tree: pidx (rows entries: point or -1), qtab (nqt entries), rtab (rows / 128 entries).
+cudaError_t tc_leaf_pass(const TcLeafPlan &L, void *ws, const float *X, const float *X2,
+                         long long npts, int d, int k, const int *pidx, int rows,
+                         const int4 *qtab, int nqt, const int2 *rtab, float *D, int *I,
+                         int ldD, int *status, cudaStream_t st);
+
 cudaError_t tc_run_prepared(const TcPlan &P, const TcCand &C, int nq, int d, int k,
                             const float *Xq, const float *Xq2, long long nrows_q,
                             const int *qidx, float *D, int *I, int ldD, void *ws, int *status,

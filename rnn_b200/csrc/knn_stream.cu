@@ -158,6 +158,10 @@ gsknn_stream_t *gsknn_stream_create(int N, int d, int k, const float *X, const f
     set_status(GSKNN_ERR_ARG, "gsknn_stream_create: invalid sizes or null pointer");
     return nullptr;
   }
+  if (shape >= 3) {  // the tensor-core batching shape works on table rows, not global ids
+    set_status(GSKNN_ERR_UNSUPPORTED, "gsknn_stream_create: CUDA-core tile shapes only");
+    return nullptr;
+  }
   StreamJob *J = new StreamJob();
   J->N = N; J->d = d; J->k = k; J->ldD = ldD; J->leaf_min = leaf_min;
   J->P = std::min(group_points, N);

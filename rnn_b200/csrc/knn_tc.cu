@@ -1573,4 +1573,149 @@ cudaError_t tc_cand_prepare_escalation(TcCand *C, void *mem, int mode, int *stat
   return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------------------------------
+// batching form: leaf panels
+// ------------------------------------------------------------------------------------------
+namespace tc {
+__global__ void iota_kernel(int *a, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    a[i] = (int)i;
+}
+}  // namespace tc
+
+int tc_leaf_tile(int d, int k, int sms) {
+  const TcPlan P = tc_plan_base(256, 256, d, k, GSKNN_TC_BF16X3, sms, false, 1);
+  return P.ok ? P.N : 0;
+}
+
+TcLeafPlan tc_leaf_plan(long long npts, int rows_cap, int d, int k, int sms) {
+  using namespace tc;
+  TcLeafPlan L{};
+  L.ok = false;
+  // the tile plan: split BF16, one split, candidate tiles of N (256 where it fits)
+  TcPlan P = tc_plan_base(256, 256, d, k, GSKNN_TC_BF16X3, sms, false, 1);
+  if (!P.ok || npts <= 0 || rows_cap <= 0 || rows_cap % TC_M != 0) return L;
+  L.rows_cap = rows_cap;
+  // per-query area for rows_cap rows, one split; smaller logs than the per-call path (a leaf
+  // offers at most a few thousand candidates; a full log overflows to the leaf brute force)
+  P.logcap = std::max(2 * P.kp, 256);
+  P.S = 1;
+  P.qtiles = L.rows_cap / TC_M;
+  P.q_pad = L.rows_cap;
+  size_t off = 0;
+  auto take = [&](size_t b) { size_t o = off; off = al256(off + b); return o; };
+  const size_t R = (size_t)L.rows_cap;
+  L.o_mu = take((size_t)d * 4);
+  L.o_mu2 = take(8);
+  L.o_stats = take(16);
+  L.o_pb = take(R * P.d_pad * 2);
+  L.o_pb_lo = take(R * P.d_pad * 2);
+  L.o_cn = take(R * 4);
+  L.o_cnrm = take(R * 4);
+  L.o_cid = take(R * 4);
+  L.o_iota = take((size_t)npts * 4);
+  P.o_pa = L.o_pb;  // the query panel is the candidate panel
+  P.o_pa_lo = L.o_pb_lo;
+  P.o_qn = L.o_cn;
+  P.o_qnrm = L.o_cnrm;
+  P.o_log = take((size_t)NPART * R * P.logcap * 8);
+  P.o_logcnt = take((size_t)NPART * R * 4);
+  P.o_kth = take((size_t)NPART * R * 4);
+  P.o_kth_shared = take(R * 4);
+  P.o_margin = take(R * 4);
+  P.o_fbl = take(R * 4);
+  P.o_fbc = take(16);
+  P.esc_mode = 0;
+  P.bytes = off;
+  L.bytes = off;
+  L.P = P;
+  L.ok = true;
+  return L;
+}
+
+int tc_leaf_tile(const TcLeafPlan &L) { return L.P.N; }
+
+cudaError_t tc_leaf_pass(const TcLeafPlan &L, void *ws, const float *X, const float *X2,
+                         long long npts, int d, int k, const int *pidx, int rows,
+                         const int4 *qtab, int nqt, const int2 *rtab, float *D, int *I,
+                         int ldD, int *status, cudaStream_t st) {
+  using namespace tc;
+  const TcPlan &P = L.P;
+  if (!L.ok || rows > L.rows_cap || rows % P.N != 0 || k > 256) return cudaErrorInvalidValue;
+  if (nqt == 0) return cudaSuccess;
+  char *base = static_cast<char *>(ws);
+  float *mu = reinterpret_cast<float *>(base + L.o_mu);
+  double *mu2 = reinterpret_cast<double *>(base + L.o_mu2);
+  unsigned *stats = reinterpret_cast<unsigned *>(base + L.o_stats);
+  void *pb = base + L.o_pb, *pb_lo = base + L.o_pb_lo;
+  float *cn = reinterpret_cast<float *>(base + L.o_cn);
+  float *cnrm = reinterpret_cast<float *>(base + L.o_cnrm);
+  uint32_t *cid = reinterpret_cast<uint32_t *>(base + L.o_cid);
+  int *iota = reinterpret_cast<int *>(base + L.o_iota);
+  int *fbc = reinterpret_cast<int *>(base + P.o_fbc);
+  cudaError_t e = cudaMemsetAsync(stats, 0, 16, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(fbc, 0, 16, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(base + P.o_kth_shared, 0xFF, (size_t)rows * 4, st);
+  if (e != cudaSuccess) return e;
+  iota_kernel<<<296, 256, 0, st>>>(iota, npts);
+  // shift: mean of a strided sample of the panel's rows (padding rows are skipped)
+  tc_center<<<(d + 31) / 32, 1024, 0, st>>>(X, d, npts, pidx, rows, std::min(rows, 4096), mu);
+  tc_mu2<<<1, 32, 0, st>>>(mu, d, mu2);
+  tc_pack<<<(rows + 7) / 8, 256, 0, st>>>(2, X, X2, d, P.d_pad, npts, pidx, rows, rows, mu, mu2,
+                                         1, pb, pb_lo, cn, cnrm, cid, stats, status, nullptr,
+                                         nullptr, nullptr, 1);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  CUtensorMap mA, mAlo, mB, mBlo;
+  e = make_panel_map(&mA, pb, P.elem, P.d_pad, rows, TC_M);
+  if (e == cudaSuccess) e = make_panel_map(&mAlo, pb_lo, P.elem, P.d_pad, rows, TC_M);
+  if (e == cudaSuccess) e = make_panel_map(&mB, pb, P.elem, P.d_pad, rows, P.N);
+  if (e == cudaSuccess) e = make_panel_map(&mBlo, pb_lo, P.elem, P.d_pad, rows, P.N);
+  if (e != cudaSuccess) return e;
+  TcParams tp{};
+  tp.Q = rows; tp.k = k; tp.nkc = P.nkc; tp.ntiles_r = rows / P.N;
+  tp.tiles_per_split = rows / P.N; tp.N = P.N; tp.NST = P.NST; tp.logcap = P.logcap;
+  tp.a_terms = P.a_terms; tp.b_terms = P.b_terms; tp.fmt = P.fmt;
+  tp.idesc = idesc_f32acc(1u, TC_M, P.N);
+  tp.cn = cn; tp.cid = cid; tp.qn = cn; tp.qnrm = cnrm; tp.stats = stats;
+  tp.Din = D; tp.ldD = ldD; tp.coefA = P.coefA; tp.coefB = P.coefB;
+  tp.log = reinterpret_cast<uint2 *>(base + P.o_log);
+  tp.logcnt = reinterpret_cast<int *>(base + P.o_logcnt);
+  tp.kth = reinterpret_cast<float *>(base + P.o_kth);
+  tp.kth_shared = reinterpret_cast<unsigned *>(base + P.o_kth_shared);
+  tp.margin = reinterpret_cast<float *>(base + P.o_margin);
+  tp.status = status;
+  tp.rowmap = pidx;
+  tp.qtab = qtab;
+  e = cudaFuncSetAttribute(tc_knn<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, P.smem);
+  if (e != cudaSuccess) return e;
+  tc_knn<2><<<nqt, NTHREADS, P.smem, st>>>(mA, mAlo, mB, mBlo, tp);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  RerankParams rp{};
+  rp.Q = rows; rp.k = k; rp.S = NPART; rp.logcap = P.logcap; rp.d = d;
+  rp.log = tp.log; rp.logcnt = tp.logcnt; rp.kth = tp.kth; rp.margin = tp.margin;
+  rp.kth_shared = tp.kth_shared;
+  rp.Xq = X; rp.Xq2 = X2; rp.Xc = X; rp.Xc2 = X2; rp.qidx = iota; rp.cid = cid;
+  rp.D = D; rp.I = I; rp.ldD = ldD;
+  rp.fallback_list = reinterpret_cast<int *>(base + P.o_fbl);
+  rp.fallback_count = fbc;
+  rp.rowmap = pidx;
+  rp.dedup = 1;
+  LeafFallbackParams fp{};
+  fp.k = k; fp.d = d; fp.N = P.N; fp.X = X; fp.X2 = X2; fp.rowmap = pidx; fp.ids = cid;
+  fp.rtab = rtab; fp.D = D; fp.I = I; fp.ldD = ldD; fp.list = rp.fallback_list;
+  fp.count = fbc;
+  const int rb = (rows + 7) / 8;
+  switch (P.kp) {
+    case 32: tc_rerank<1><<<rb, 256, 0, st>>>(rp); tc_fallback_leaf<1><<<148, 256, 0, st>>>(fp); break;
+    case 64: tc_rerank<2><<<rb, 256, 0, st>>>(rp); tc_fallback_leaf<2><<<148, 256, 0, st>>>(fp); break;
+    case 128: tc_rerank<4><<<rb, 256, 0, st>>>(rp); tc_fallback_leaf<4><<<148, 256, 0, st>>>(fp); break;
+    case 256: tc_rerank<8><<<rb, 256, 0, st>>>(rp); tc_fallback_leaf<8><<<148, 256, 0, st>>>(fp); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 }  // namespace gsknn

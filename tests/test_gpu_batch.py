@@ -66,7 +66,7 @@ def _assert_unique_rows(I):
         assert np.unique(real).size == real.size
 
 
-@pytest.mark.parametrize("shape", [0, 1, 2])
+@pytest.mark.parametrize("shape", [0, 1, 2, 3])
 def test_batch_exact_integer_data_every_shape(oracle, shape):
     N, d, k, T = 5000, 8, 16, 3
     X = _int_table(900, N, d)
@@ -92,8 +92,8 @@ def test_batch_autotuned_gaussian_mixture(oracle):
     passes = [lv.select_trees(range(0, T)), lv.select_trees(range(T, 2 * T))]
     B.forget_tuning()
     D, I, info = _run(X, X2, k, passes, -1, T, 100)
-    assert info["shape"] in (0, 1, 2)
-    assert len(info["tune_ms"]) == 3 and min(info["tune_ms"].values()) > 0
+    assert info["shape"] in (0, 1, 2, 3)
+    assert len(info["tune_ms"]) == 4 and min(info["tune_ms"].values()) > 0
     assert is_maxheap(D)
     _assert_unique_rows(I)
     ptr, pts = _leaves_concat(passes)
@@ -126,7 +126,7 @@ def test_batch_partial_trees_tiny_leaves_and_k_above_leaf(oracle):
     for s in sizes1:
         pts.append(perm1[off:off + s]); off += s; ptr.append(ptr[-1] + s); tree.append(1)
     lv = B.Leaves(np.asarray(ptr, np.int32), np.concatenate(pts), np.asarray(tree, np.int32))
-    for shape in (0, 1):
+    for shape in (0, 1, 3):
         D, I, _ = _run(X, X2, k, [lv], shape, 2, 1)
         assert is_maxheap(D)
         _assert_unique_rows(I)
@@ -137,8 +137,11 @@ def test_batch_partial_trees_tiny_leaves_and_k_above_leaf(oracle):
         assert np.all(np.isinf(Ds[~np.isfinite(De)]))
 
 
-def test_batch_graph_replays_many_passes(oracle):
-    """Four passes through one captured graph, checked after every pass."""
+@pytest.mark.parametrize("shape", [1, 3])
+def test_batch_graph_replays_many_passes(oracle, shape):
+    """Four passes (for the CUDA-core shape through one captured graph; for the tensor-core
+    shape tree by tree, each re-rank merging into the heap without entering an id twice),
+    checked after every pass."""
     import torch
     N, d, k, T = 8000, 10, 24, 2
     X = _int_table(930, N, d)
@@ -146,7 +149,7 @@ def test_batch_graph_replays_many_passes(oracle):
     lv = B.rkdt_leaves(X, 4 * T, 80, 320, seed=931)
     Xd, X2d = _dev(X, X2)
     D, I = _heap(N, k)
-    job = B.BatchJob(Xd, X2d, D, I, k, trees_per_pass=T, leaf_min=80, shape=1)
+    job = B.BatchJob(Xd, X2d, D, I, k, trees_per_pass=T, leaf_min=80, shape=shape)
     done = []
     for p in range(4):
         lp = lv.select_trees(range(p * T, (p + 1) * T))
@@ -162,7 +165,8 @@ def test_batch_graph_replays_many_passes(oracle):
     torch.cuda.synchronize()
 
 
-def test_batch_merges_into_an_existing_heap(oracle):
+@pytest.mark.parametrize("shape", [0, 3])
+def test_batch_merges_into_an_existing_heap(oracle, shape):
     """Heaps first filled by sgsknn (FP32 mode, random candidates), then refined by two passes."""
     N, d, k, T = 4000, 8, 16, 2
     X = _int_table(940, N, d)
@@ -179,7 +183,7 @@ def test_batch_merges_into_an_existing_heap(oracle):
         G.set_mode(prev)
     lv = B.rkdt_leaves(X, 2 * T, 64, 256, seed=942)
     passes = [lv.select_trees(range(0, T)), lv.select_trees(range(T, 2 * T))]
-    D, I, _ = _run(X, X2, k, passes, 0, T, 64, D0, I0)
+    D, I, _ = _run(X, X2, k, passes, shape, T, 64, D0, I0)
     _assert_unique_rows(I)
     ptr, pts = _leaves_concat(passes)
     De, Ie = oracle.allnn_leaves(k, X, X2, ptr, pts, D0, I0)
@@ -188,7 +192,8 @@ def test_batch_merges_into_an_existing_heap(oracle):
     assert np.array_equal(Ds, De)
 
 
-def test_batch_reports_a_point_outside_the_table():
+@pytest.mark.parametrize("shape", [1, 3])
+def test_batch_reports_a_point_outside_the_table(shape):
     N, d, k = 1000, 4, 8
     X = _int_table(950, N, d)
     X2 = W.sq_norms(X)
@@ -197,8 +202,28 @@ def test_batch_reports_a_point_outside_the_table():
     lv = B.Leaves(np.array([0, 500, N], np.int32), pts, np.array([0, 0], np.int32))
     Xd, X2d = _dev(X, X2)
     D, I = _heap(N, k)
-    job = B.BatchJob(Xd, X2d, D, I, k, trees_per_pass=1, leaf_min=100, shape=1)
+    job = B.BatchJob(Xd, X2d, D, I, k, trees_per_pass=1, leaf_min=100, shape=shape)
     job.run_pass(lv)
     with pytest.raises(G.GsknnError):
         job.sync()
     job.close()
+
+
+def test_batch_tensor_core_shape_gaussian_mixture(oracle):
+    """The tensor-core shape on clustered data (d = 64, k = 32, leaves of 256..2048 points, two
+    passes of four trees): exact FP64 neighbour sets, distances the FP64 values in float."""
+    N, d, k, T = 30000, 64, 32, 4
+    X = W.gaussian_mixture_table(960, N, d, dtype=np.float32)
+    X2 = W.sq_norms(X)
+    lv = B.rkdt_leaves(X, 2 * T, 256, 2048, seed=961)
+    passes = [lv.select_trees(range(0, T)), lv.select_trees(range(T, 2 * T))]
+    D, I, info = _run(X, X2, k, passes, 3, T, 256)
+    assert info["shape"] == 3
+    assert is_maxheap(D)
+    _assert_unique_rows(I)
+    ptr, pts = _leaves_concat(passes)
+    De, Ie = oracle.allnn_leaves(k, X, X2, ptr, pts)
+    bad = [j for j in range(N) if not np.array_equal(np.sort(I[j]), np.sort(Ie[j]))]
+    assert not bad, bad[:5]
+    Ds = np.sort(D.astype(np.float64), axis=1)
+    assert np.all(np.abs(Ds - De) <= 1e-6 * np.abs(De) + 1e-9)
