@@ -142,6 +142,9 @@ def cpu_worker(spec: str) -> None:
     if cfg.get("kind") == "config1":
         config1_cpu_worker(cfg, nthreads)
         return
+    if cfg.get("kind") in ("config3", "config5"):
+        slice_cpu_worker(cfg, nthreads)
+        return
     p = W.config2(seed=cfg["seed"])
     ref_so = os.path.join(ROOT, "oracle", "_ref", "libgsknn_ref.so")
     kind = "reference" if os.path.exists(ref_so) else "port"
@@ -237,6 +240,56 @@ def config1_cpu_worker(cfg, nthreads) -> None:
     print("CPUJSON " + json.dumps({"value": 2.0 * p.n * p.m / t, "ms_per_step": 1e3 * t,
                                    "steps": len(times), "kind": "reference",
                                    "threads": nthreads}), flush=True)
+
+
+def slice_cpu_worker(cfg, nthreads) -> None:
+    """The reference's sgsknn_var1 on a query slice of the precision-form workload (config 3:
+    262,144 latent-manifold references, d = 256, k = 64) or of the serving workload (config 5:
+    4,194,304 resident U[0,1) references, d = 128, k = 64): one block of 104 queries per thread
+    (the reference spreads its query blocks over the threads), one call."""
+    from rnn_b200 import workloads as W
+    from oracle.oracle import ReferenceLib
+    ref_so = os.path.join(ROOT, "oracle", "_ref", "libgsknn_ref.so")
+    R = ReferenceLib(ref_so)
+    q = 104 * nthreads
+    if cfg["kind"] == "config3":
+        p = W.config3(seed=3)
+        X, X2, alpha, k = p.X, p.X2, p.alpha, p.k
+        beta = np.ascontiguousarray(p.beta[:q])
+    else:
+        nref, d, k = 1 << 22, 128, 64
+        X = np.empty((nref + q, d), dtype=np.float32)
+        X[:nref] = W.uniform_table(71, nref, d, np.float32)
+        X[nref:] = W.uniform_table(72, q, d, np.float32)
+        X2 = W.sq_norms(X)
+        alpha = np.arange(nref, dtype=np.int32)
+        beta = np.arange(nref, nref + q, dtype=np.int32)
+    D = np.full((q, k), 1.79e30, dtype=np.float32)
+    I = np.full((q, k), -1, dtype=np.int32)
+    t0 = time.perf_counter()
+    R.var1(k, X, X2, beta, X, X2, alpha, D, I)
+    t = time.perf_counter() - t0
+    print("CPUJSON " + json.dumps({"value": float(q) * alpha.size / t, "seconds": t,
+                                   "queries": q, "references": int(alpha.size), "k": k,
+                                   "kind": "reference", "threads": nthreads}), flush=True)
+
+
+def slice_cpu_baseline(kind: str, threads: int) -> dict:
+    spec = json.dumps({"kind": kind, "threads": threads})
+    env = dict(os.environ)
+    env["CUDA_VISIBLE_DEVICES"] = ""
+    r = subprocess.run([sys.executable, os.path.abspath(__file__), "--cpu-worker", spec],
+                       capture_output=True, text=True, env=env, timeout=900)
+    for line in r.stdout.splitlines():
+        if line.startswith("CPUJSON "):
+            o = json.loads(line[8:])
+            return {"value": o["value"], "unit": "distance-evals/s", "cores": o["threads"],
+                    "kind": o["kind"],
+                    "sample": (f"reference sgsknn_var1, {o['queries']} queries x "
+                               f"{o['references']} references, k={o['k']}, one call, "
+                               f"{o['seconds']:.1f} s, GSKNN_IC_NT=OMP_NUM_THREADS="
+                               f"{o['threads']}")}
+    raise RuntimeError(kind + " cpu baseline failed:\n" + r.stdout[-2000:] + r.stderr[-2000:])
 
 
 def config1_cpu_baseline(seconds: float, threads: int) -> dict:
@@ -796,6 +849,11 @@ def precision_form(L, G, W, dev, peaks, args):
         for nm in ("tf32", "bf16", "bf16x3"):
             if nm in res:
                 res[nm]["speedup_vs_plain_fp32"] = res[nm]["value"] / base
+    if not args.precision_only and not args.no_cpu_baseline:
+        try:
+            res["cpu_baseline"] = slice_cpu_baseline("config3", args.threads)
+        except Exception as e:  # reported, not fatal
+            res["cpu_baseline"] = {"error": str(e)[-400:]}
     del prob
     torch.cuda.empty_cache()
     return res
@@ -1037,6 +1095,13 @@ def serving_form(L, G, W, dev, args):
     res["speedup_vs_per_request_fp32"] = res["value"] / res["per_request_fp32"]["value"]
     del Rd, R2d
     torch.cuda.empty_cache()
+    if not args.no_cpu_baseline:
+        try:  # the reference's sgsknn on a request-sized query slice against the resident set
+            cb = slice_cpu_baseline("config5", args.threads)
+            cb["mean_request_ms"] = float(ms.mean()) * nref / cb["value"] * 1e3
+            res["cpu_baseline"] = cb
+        except Exception as e:  # reported, not fatal
+            res["cpu_baseline"] = {"error": str(e)[-400:]}
     return res
 
 
@@ -1184,6 +1249,7 @@ def summarize(out: dict) -> dict:
                                      "rows_exact": (pf[nm].get("accuracy") or {}).get(
                                          "rows_exact_fp64_recall")}
                                 for nm in ("fp32", "tf32", "bf16", "bf16x3") if nm in pf}
+        sm["precision_form"]["cpu_evals_per_s"] = r((pf.get("cpu_baseline") or {}).get("value"))
     c1 = out.get("fp64_config1")
     if c1:
         sm["fp64_config1"] = {"evals_per_s": r(c1["value"]), "ms": r(c1["ms_per_step"]),
@@ -1200,7 +1266,10 @@ def summarize(out: dict) -> dict:
     if sv:
         lat = sv.get("latency_ms") or {}
         sm["serving"] = {"p50_ms": r(lat.get("p50")), "p99_ms": r(lat.get("p99")),
-                         "evals_per_s": r(sv.get("value"))}
+                         "evals_per_s": r(sv.get("value")),
+                         "cpu_evals_per_s": r((sv.get("cpu_baseline") or {}).get("value")),
+                         "cpu_mean_request_ms": r((sv.get("cpu_baseline") or {}).get(
+                             "mean_request_ms"))}
     cb = out.get("cpu_baseline")
     if isinstance(cb, dict) and "value" in cb:
         sm["cpu_baseline_evals_per_s"] = r(cb["value"])
