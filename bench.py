@@ -108,7 +108,7 @@ def parse():
                     help="mean request arrival rate (requests/s, Poisson)")
     ap.add_argument("--kernel-case", default=None,
                     choices=["config1", "large_k", "tc_q8192", "batch_small", "serve_one",
-                             "fp32_q8192"],
+                             "fp32_q8192", "batch_small_tc"],
                     help="one small run of one path, for per-kernel profiling: warm-up call, "
                          "then the profiled call")
     ap.add_argument("--cpu-worker", default=None, help=argparse.SUPPRESS)
@@ -1155,7 +1155,7 @@ def kernel_case(name: str) -> dict:
       tc_q8192    split BF16 on 8,192 headline queries (tc_pack, tc_knn, tc_rerank)
       fp32_q8192  plain FP32 on 8,192 headline queries (fused_knn_simt<float>)
       batch_small one pass of 8 trees over 262,144 mixture points (batch_pack, batch_knn_simt,
-                  batch_merge)
+                  batch_merge); batch_small_tc the same in the tensor-core shape
       serve_one   one 512-row request against 1,048,576 resident points (query_norms,
                   scatter, the tensor-core kernels)"""
     import torch
@@ -1188,14 +1188,15 @@ def kernel_case(name: str) -> dict:
         p = W.config2()
         beta = np.ascontiguousarray(p.beta[:8192])
         dev_call(p.X, p.X2, p.alpha, beta, p.k, mode=1 if name == "fp32_q8192" else 0)
-    elif name == "batch_small":
+    elif name in ("batch_small", "batch_small_tc"):
         from rnn_b200 import batch as B
         p = W.config4(n_points=1 << 18, passes=1)
         lv = B.rkdt_leaves(p.X, p.trees_per_pass, p.leaf_min, p.leaf_max, seed=p.tree_seed)
         Xd, X2d = torch.from_numpy(p.X).to(dev), torch.from_numpy(p.X2).to(dev)
         D = torch.full((p.N, p.k), float("inf"), device=dev)
         I = torch.full((p.N, p.k), -1, dtype=torch.int32, device=dev)
-        job = B.BatchJob(Xd, X2d, D, I, p.k, p.trees_per_pass, p.leaf_min, shape=2,
+        job = B.BatchJob(Xd, X2d, D, I, p.k, p.trees_per_pass, p.leaf_min,
+                         shape=3 if name == "batch_small_tc" else 2,
                          stream=torch.cuda.current_stream(dev))
         for _ in range(2):
             job.run_pass(lv)
