@@ -386,6 +386,7 @@ struct BatchJob {
   int2 *h_tc_rtab;
   long long tc_cap_rows;        // capacity (rows over all trees) of the arrays above
   long long *h_tc_tree;         // per tree: rows, query tiles, and the offsets of the three
+  bool tc_setup_done;           // the workspace holds the row map and the shift
   float *tD;                    // scratch heap for timing the tensor-core shape
   int *tI;
   float tune_tc_ms;
@@ -560,6 +561,7 @@ static void free_tc(BatchJob *b) {
   b->h_tc_rtab = nullptr;
   b->tc_cap_rows = 0;
   b->tcl.ok = false;
+  b->tc_setup_done = false;
 }
 
 // Workspace and plan arrays for `rows` panel rows over all trees, `tree_rows` for one tree (with
@@ -612,7 +614,9 @@ static int enqueue_tc_pass(BatchJob *b, float *D, int *I) {
     if (tr[1] == 0) continue;
     BCU(gsknn::tc_leaf_pass(b->tcl, b->tc_ws, b->X, b->X2, b->N, b->d, b->k,
                             b->tc_pidx + tr[2], (int)tr[0], b->tc_qtab + tr[3], (int)tr[1],
-                            b->tc_rtab + tr[4], D, I, b->ldD, b->status, b->st));
+                            b->tc_rtab + tr[4], D, I, b->ldD, b->status, b->st,
+                            !b->tc_setup_done));
+    b->tc_setup_done = true;
   }
   return GSKNN_OK;
 }

@@ -191,11 +191,12 @@ struct TcLeafPlan {
 TcLeafPlan tc_leaf_plan(long long npts, int rows_cap, int d, int k, int sms);
 // Candidate tile width of the leaf panels: every leaf starts at a multiple of it (0: no plan).
 int tc_leaf_tile(int d, int k, int sms);
-// One tree: pidx (rows entries: point or -1), qtab (nqt entries), rtab (rows / 128 entries).
+// One tree: pidx (rows entries: point or -1), qtab (nqt entries), rtab (rows / 128 entries);
+// `setup` on the first call after the workspace was allocated (row index map and shift).
 cudaError_t tc_leaf_pass(const TcLeafPlan &L, void *ws, const float *X, const float *X2,
                          long long npts, int d, int k, const int *pidx, int rows,
                          const int4 *qtab, int nqt, const int2 *rtab, float *D, int *I,
-                         int ldD, int *status, cudaStream_t st);
+                         int ldD, int *status, cudaStream_t st, bool setup);
 
 cudaError_t tc_run_prepared(const TcPlan &P, const TcCand &C, int nq, int d, int k,
                             const float *Xq, const float *Xq2, long long nrows_q,

@@ -1639,7 +1639,7 @@ int tc_leaf_tile(const TcLeafPlan &L) { return L.P.N; }
 cudaError_t tc_leaf_pass(const TcLeafPlan &L, void *ws, const float *X, const float *X2,
                          long long npts, int d, int k, const int *pidx, int rows,
                          const int4 *qtab, int nqt, const int2 *rtab, float *D, int *I,
-                         int ldD, int *status, cudaStream_t st) {
+                         int ldD, int *status, cudaStream_t st, bool setup) {
   using namespace tc;
   const TcPlan &P = L.P;
   if (!L.ok || rows > L.rows_cap || rows % P.N != 0 || k > 256) return cudaErrorInvalidValue;
@@ -1658,10 +1658,14 @@ cudaError_t tc_leaf_pass(const TcLeafPlan &L, void *ws, const float *X, const fl
   if (e == cudaSuccess) e = cudaMemsetAsync(fbc, 0, 16, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(base + P.o_kth_shared, 0xFF, (size_t)rows * 4, st);
   if (e != cudaSuccess) return e;
-  iota_kernel<<<296, 256, 0, st>>>(iota, npts);
-  // shift: mean of a strided sample of the panel's rows (padding rows are skipped)
-  tc_center<<<(d + 31) / 32, 1024, 0, st>>>(X, d, npts, pidx, rows, std::min(rows, 4096), mu);
-  tc_mu2<<<1, 32, 0, st>>>(mu, d, mu2);
+  if (setup) {
+    // once per workspace: the row index map, and the shift (mean of a strided sample of the
+    // first panel's rows, padding skipped), which serves every later tree of the same table
+    iota_kernel<<<296, 256, 0, st>>>(iota, npts);
+    tc_center<<<(d + 31) / 32, 1024, 0, st>>>(X, d, npts, pidx, rows, std::min(rows, 4096),
+                                              mu);
+    tc_mu2<<<1, 32, 0, st>>>(mu, d, mu2);
+  }
   tc_pack<<<(rows + 7) / 8, 256, 0, st>>>(2, X, X2, d, P.d_pad, npts, pidx, rows, rows, mu, mu2,
                                          1, pb, pb_lo, cn, cnrm, cid, stats, status, nullptr,
                                          nullptr, nullptr, 1);
