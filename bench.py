@@ -1149,7 +1149,8 @@ def e2e_host(L, G, p, beta_h, args):
 
 def kernel_case(name: str) -> dict:
     """One small invocation of one path (a warm-up call, then the call to profile), so that an
-    ncu capture of any of the library's kernels can be taken on a small case:
+    ncu capture of any of the library's kernels can be taken on a small case; `last_ms` is the
+    stream time of the profiled call (CUDA events around it):
       config1     dgsknn FP64 (pack_panels, fused_knn_simt<double>, finalize_heap)
       large_k     k = 600 float (dist_block, select_rows)
       tc_q8192    split BF16 on 8,192 headline queries (tc_pack, tc_knn, tc_rerank)
@@ -1164,6 +1165,8 @@ def kernel_case(name: str) -> dict:
     dev = torch.device("cuda:0")
     torch.cuda.set_device(dev)
     t = time.perf_counter()
+    # device time of the last (profiled) call or pass
+    ev = [torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)]
 
     def dev_call(X, X2, alpha, beta, k, mode=0, reps=2):
         Xd, X2d = torch.from_numpy(X).to(dev), torch.from_numpy(X2).to(dev)
@@ -1174,7 +1177,9 @@ def kernel_case(name: str) -> dict:
         for _ in range(reps):
             D.fill_(float("inf"))
             I.fill_(-1)
+            ev[0].record()
             G.knn_device(Xd, X2d, a, Xd, X2d, b, D, I)
+            ev[1].record()
         torch.cuda.synchronize()
         G.set_mode(0)
 
@@ -1199,7 +1204,9 @@ def kernel_case(name: str) -> dict:
                          shape=3 if name == "batch_small_tc" else 2,
                          stream=torch.cuda.current_stream(dev))
         for _ in range(2):
+            ev[0].record()
             job.run_pass(lv)
+            ev[1].record()
         job.sync()
     elif name == "serve_one":
         from rnn_b200 import serve as SV
@@ -1209,11 +1216,15 @@ def kernel_case(name: str) -> dict:
         srv = SV.Server(Rd, R2d, mode=0, max_batch_queries=1024, max_k=64, slots=1)
         Q = W.uniform_table(62, 512, 128, np.float32)
         for _ in range(2):
+            ev[0].record()
             rid = srv.submit(Q, 64)
             srv.wait(rid)
             srv.release(rid)
+            ev[1].record()
         srv.close()
-    return {"kernel_case": name, "seconds": time.perf_counter() - t}
+    torch.cuda.synchronize()
+    return {"kernel_case": name, "seconds": time.perf_counter() - t,
+            "last_ms": ev[0].elapsed_time(ev[1])}
 
 def summarize(out: dict) -> dict:
     """Compact figures of every leg, placed last in the JSON line so that a reader keeping only

@@ -157,9 +157,10 @@ const char *gsknn_last_error_string(void);
  *   GSKNN_MODE_FP32 -- CUDA-core FP32 distances;
  *   GSKNN_MODE_TF32, GSKNN_MODE_BF16 -- tensor-core distances with an FP64 re-rank of every
  *     candidate within the rounding bound of the k-th distance (exact index sets);
- *   GSKNN_MODE_AUTO -- split BF16 where its tiles fit in shared memory (the narrowest re-rank
- *     band; measured fastest of the exact forms at d = 64 and 256), else TF32, else FP32
- *     (default). */
+ *   GSKNN_MODE_AUTO -- from d = 128, BF16 (queries whose re-rank band overflows its log run
+ *     again in split BF16); below d = 128, split BF16 (the narrowest band; plain BF16 overflows
+ *     there); TF32 where neither fits in shared memory; else FP32 (default). Each choice was
+ *     measured fastest of the exact forms on the d = 64 and d = 256 workloads. */
 #define GSKNN_MODE_AUTO 0
 #define GSKNN_MODE_FP32 1
 #define GSKNN_MODE_TF32 2

@@ -463,12 +463,15 @@ static int knn_device_tc(int mode, int nq, int nc, int d, int k, const float *Xq
 }
 
 // The arithmetic used for a float call: explicit modes are honoured; AUTO takes the
-// tensor-core form with the exact FP64 re-rank where it fits (split BF16 below d = 128, TF32
-// from there), else the CUDA-core FP32 kernel.
+// tensor-core form with the exact FP64 re-rank where it fits (split BF16 below d = 128, BF16
+// from there, TF32 where neither fits), else the CUDA-core FP32 kernel.
 static int pick_mode(int nq, int nc, int d, int k) {
   if (g_mode != GSKNN_MODE_AUTO) return g_mode;
-  // split BF16 keeps the re-rank band narrowest (input error ~u^2) and measured fastest of the
-  // exact forms at d = 64 and d = 256; TF32 where its larger query tile does not fit
+  // Split BF16 keeps the re-rank band narrowest (input error ~u^2): at d = 64 plain BF16's band
+  // overflows the logs and most queries run again. From d = 128 one BF16 MMA per product was
+  // measured fastest (d = 256: 10.8 ms against 13.9 ms in split BF16 for 32,768 x 262,144,
+  // k = 64); the few queries whose log overflows run again in split BF16.
+  if (d >= 128 && tc_plan(nq, nc, d, k, GSKNN_TC_BF16, sm_count()).ok) return GSKNN_TC_BF16;
   if (tc_plan(nq, nc, d, k, GSKNN_TC_BF16X3, sm_count()).ok) return GSKNN_TC_BF16X3;
   if (tc_plan(nq, nc, d, k, GSKNN_TC_TF32, sm_count()).ok) return GSKNN_TC_TF32;
   return GSKNN_MODE_FP32;

@@ -117,8 +117,8 @@ struct TcPlan {
   float coefA, coefB;
   // query-side workspace offsets (absolute within the workspace; they start after the
   // prepared-candidate area when the plan includes it)
-  size_t o_pa, o_pa_lo, o_qn, o_qnrm, o_log, o_logcnt, o_kth, o_kth_shared, o_margin, o_fbl,
-      o_fbc;
+  size_t o_pa, o_pa_lo, o_qn, o_qnrm, o_log, o_logcnt, o_proot, o_margin, o_fbl, o_fbc;
+  int hk;  // partition bound: heap entries per row and epilogue part
   size_t cand_bytes;  // prepared-candidate area at the start of the workspace (0: separate)
   // Escalation: queries whose band log overflowed in this format run again in a narrower one
   // (esc_mode, 0 = none: they go straight to the FP64 brute force). Its query-side workspace

@@ -12,9 +12,11 @@
 //                 running maxima for the bound
 //   tc_knn        warp 0 TMA producer, warp 1 MMA issuer (TMEM owner), warps 2-9 epilogue (two
 //                 per TMEM lane quarter, each taking half of every tile's columns) with
-//                 one query row per thread: approximate d' = qn' + cn' - 2<q~,c~>, a per-query
-//                 max-heap of the k smallest d' in shared memory (threshold), and a per-query
-//                 log in HBM of every candidate with d' <= k-th + 2E
+//                 one query row per thread: approximate d' = qn' + cn' - 2<q~,c~>; per row and
+//                 epilogue part a max-heap of the hk smallest d' of its own columns in shared
+//                 memory, where hk = ceil(k / (parts in a window of up to 4 splits)), so that the
+//                 largest root of a window bounds the k-th from above (threshold = that + 2E);
+//                 a per-query log in HBM of every candidate under the threshold
 //   tc_rerank     one warp per query: exact FP64 distances of the logged band, sorted merge with
 //                 the incoming heap row, descending write-back (a valid max-heap)
 //   tc_fallback   queries whose log overflowed: exact FP64 brute force over all candidates
@@ -41,8 +43,8 @@ constexpr int TC_M = 128;            // queries per CTA (TMEM lanes)
 constexpr int CHUNK_BYTES = 128;     // K bytes per TMA box / swizzle atom row
 constexpr int A_CHUNK = TC_M * CHUNK_BYTES;  // 16 KB
 // Warp 0 TMA producer, warp 1 MMA issuer, then NEPI epilogue warps: NPART per TMEM lane quarter,
-// part j of a quarter taking the j-th of NPART equal column ranges of every tile. Part 0 keeps
-// the rows' heaps; the other parts log only and take the heap root as their threshold.
+// part j of a quarter taking the j-th of NPART equal column ranges of every tile. Every part keeps
+// a small heap of its own columns per row (the partition bound, see TcParams::proot).
 constexpr int NEPI = TC_EPI_WARPS;
 constexpr int NPART = TC_EPI_PARTS;
 constexpr int NTHREADS = 32 * (2 + NEPI);
@@ -191,7 +193,7 @@ __global__ void __launch_bounds__(256) tc_pack(
 // the tensor-core kernel
 // ------------------------------------------------------------------------------------------
 struct TcParams {
-  int Q, k, nkc, ntiles_r, tiles_per_split, N, NST, logcap;
+  int Q, k, nkc, ntiles_r, N, NST, logcap;
   int a_terms, b_terms, fmt;
   uint32_t idesc;
   const float *cn;
@@ -204,8 +206,15 @@ struct TcParams {
   float coefA, coefB;
   uint2 *log;
   int *logcnt;
-  float *kth;
-  unsigned *kth_shared;  // per query: best k-th approximate distance over splits (float bits)
+  // Partition bound. A query's candidates fall into P = NPART * S partitions (split, part). Each
+  // keeps a heap of the hk = ceil(k / NPART) smallest approximate distances among its own
+  // candidates seen so far, and publishes its root at proot[query * P + split * NPART + part]
+  // (bits of max(root, 0); all bits set while the heap is not full). Any NPART heaps hold at
+  // least k real candidates, so the NPART-th smallest root among any partitions of the query --
+  // those of its own CTA, and of up to W - 1 other splits as far as they have run -- bounds the
+  // query's k-th from above.
+  unsigned *proot;
+  int hk, W, S;
   float *margin;
   int *status;
   float *dbg;
@@ -229,8 +238,14 @@ struct SmemLayout {
   uint32_t a_off, b_off, heap_off, cn_off, bar_off, tmem_off, total;
 };
 
+// Partition bound (see TcParams::proot): heap entries per row and part, and the splits whose
+// published roots a row reads (its own and up to three more).
+__host__ __device__ inline int tc_heap_k(int k) { return (k + NPART - 1) / NPART; }
+__host__ __device__ inline int tc_window(int S) { return S < 4 ? S : 4; }
+
+// heap_row: heap entries per row over all epilogue parts
 __host__ __device__ inline SmemLayout tc_smem_layout(int nkc, int a_terms, int b_terms, int N,
-                                                     int NST, int k) {
+                                                     int NST, int heap_row) {
   SmemLayout L;
   uint32_t off = 0;
   L.a_off = off;
@@ -238,7 +253,7 @@ __host__ __device__ inline SmemLayout tc_smem_layout(int nkc, int a_terms, int b
   L.b_off = off;
   off += (uint32_t)NST * b_terms * N * CHUNK_BYTES;
   L.heap_off = off;
-  off += (uint32_t)k * TC_M * 4;
+  off += (uint32_t)heap_row * TC_M * 4;
   off = (off + 15) & ~15u;
   L.cn_off = off;  // candidate norms of the tiles in flight, copied by the MMA warp
   off += (uint32_t)CN_SLOTS * N * 4;
@@ -252,7 +267,9 @@ __host__ __device__ inline SmemLayout tc_smem_layout(int nkc, int a_terms, int b
 }
 
 struct EpiState {
-  float qn, E2, thr0, root, shared, thr, Tv;
+  // root: this part's heap root; o1 <= o2: the two smallest roots among the other partitions
+  // the row reads (as last published); pub: what this part last published
+  float qn, E2, thr0, root, o1, o2, pub, thr, Tv;
   int cnt;
   int ovf;
   // optional diagnostics: logged candidates, heap inserts, convergent-loop iterations, chunks
@@ -260,11 +277,11 @@ struct EpiState {
   unsigned n_ev, n_ins, n_it, n_sc;
 };
 
-// The k-th smallest approximate distance of any subset of the candidates bounds the global one
-// from above, so the threshold uses the smaller of this split's own k-th and the best one any
-// split of the query has published.
+// Any two partitions' heaps hold at least k real candidates, so the second smallest root among
+// this part's and the others' bounds the query's k-th smallest approximate distance from above.
 __device__ __forceinline__ void refresh_threshold(EpiState &s) {
-  float t = fminf(s.root, s.shared) + s.E2;
+  static_assert(NPART == 2, "the bound takes the NPART-th smallest root");
+  float t = fminf(fmaxf(s.root, s.o1), s.o2) + s.E2;
   s.thr = t < s.thr0 ? t : s.thr0;
   // padding rows past the last query never admit; nor does a row whose log overflowed (the
   // query is finished by a later pass), so its chunks stop taking the slow path
@@ -321,12 +338,12 @@ __device__ __forceinline__ void epi_defer(float dp, bool ins, float (&pend)[PEND
   np += ins ? 1 : 0;
 }
 
-// One candidate of the exact slow path: log it (when `act` and under the threshold) and, for
-// heap owners, defer its heap insert. Branch-free: every lane of the warp runs it, with
-// predicates instead of divergent branches.
+// One candidate of the exact slow path: log it (when `act` and under the threshold) and defer
+// its heap insert. Branch-free: every lane of the warp runs it, with predicates instead of
+// divergent branches.
 __device__ __forceinline__ void epi_candidate(EpiState &s, float v, uint32_t id, bool act,
-                                              uint2 *lg, int logcap, bool owner,
-                                              float (&pend)[PEND], int &np) {
+                                              uint2 *lg, int logcap, float (&pend)[PEND],
+                                              int &np) {
   const float dp = v + s.qn;
   const bool take = act && dp <= s.thr;
   s.n_ev += take ? 1u : 0u;
@@ -334,13 +351,13 @@ __device__ __forceinline__ void epi_candidate(EpiState &s, float v, uint32_t id,
   if (take && !s.ovf && room) lg[s.cnt] = make_uint2(__float_as_uint(dp), id);
   s.cnt += (take && !s.ovf && room) ? 1 : 0;
   s.ovf |= (take && !room) ? 1 : 0;
-  epi_defer(dp, take && owner && dp < s.root, pend, np);
+  epi_defer(dp, take && dp < s.root, pend, np);
 }
 
 // Apply the deferred inserts (all lanes of the warp together, so their sift-downs overlap),
-// publish the new k-th to the other splits and tighten the threshold.
+// publish the new root to the other partitions and tighten the threshold.
 __device__ __forceinline__ void epi_flush(EpiState &s, float *heap, int row, int k,
-                                          float (&pend)[PEND], int &np, unsigned *ksh) {
+                                          float (&pend)[PEND], int &np, unsigned *pslot) {
 #pragma unroll
   for (int j = 0; j < PEND; j++) {
     if (j < np && pend[j] < s.root) {
@@ -349,10 +366,12 @@ __device__ __forceinline__ void epi_flush(EpiState &s, float *heap, int row, int
     }
   }
   np = 0;
-  // non-negative floats order like their bit patterns
-  if (s.root >= 0.0f && s.root < s.shared) {
-    atomicMin(ksh, __float_as_uint(s.root));
-    s.shared = s.root;
+  // published as non-negative float bits (a larger value bounds as well), which order like
+  // unsigned integers; only this partition writes its slot
+  const float pv = fmaxf(s.root, 0.0f);
+  if (pv < s.pub) {
+    __stcg(pslot, __float_as_uint(pv));
+    s.pub = pv;
   }
   refresh_threshold(s);
 }
@@ -366,10 +385,13 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   // escalation pass: launched for the largest possible query count, the tiles past the count
   // on the device exit before any set-up
   const int Qn = p.dQ ? *p.dQ : p.Q;
+  // grid: (query tile, split), query tiles fastest, so that a query's later splits mostly start
+  // after its first ones finished and take their final roots as a tight bound from the first
+  // tile; or one block per qtab entry
   if (!p.qtab && (int)blockIdx.x * TC_M >= Qn) return;
   const uint32_t raw = su32(smem_raw);
   unsigned char *smem = smem_raw + ((1024u - (raw & 1023u)) & 1023u);
-  const SmemLayout L = tc_smem_layout(p.nkc, p.a_terms, p.b_terms, p.N, p.NST, p.k);
+  const SmemLayout L = tc_smem_layout(p.nkc, p.a_terms, p.b_terms, p.N, p.NST, NPART * p.hk);
   unsigned char *sA = smem + L.a_off;
   unsigned char *sB = smem + L.b_off;
   float *heap = reinterpret_cast<float *>(smem + L.heap_off);
@@ -392,8 +414,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     t_begin = w.y;
     t_end = w.z;
   } else {
-    t_begin = split * p.tiles_per_split;
-    t_end = t_begin + p.tiles_per_split;
+    // balanced ranges: every split gets floor or ceil of ntiles_r / S tiles
+    t_begin = (int)((long long)split * p.ntiles_r / p.S);
+    t_end = (int)((long long)(split + 1) * p.ntiles_r / p.S);
   }
   if (t_end > p.ntiles_r) t_end = p.ntiles_r;
   const int ntile = t_end > t_begin ? t_end - t_begin : 0;
@@ -417,9 +440,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     tmem_alloc(tmem_holder, (uint32_t)(2 * N));
     tmem_relinquish();
   }
-  // the per-row heaps start at +inf before any epilogue warp reads a root (the log-only warp of
-  // a row reads its owner's root as a threshold)
-  for (int i = threadIdx.x; i < p.k * TC_M; i += NTHREADS) heap[i] = Num<float>::inf();
+  // the per-row heaps start at +inf before any epilogue warp reads a root (each part of a lane
+  // quarter reads the other's root as part of its bound)
+  for (int i = threadIdx.x; i < NPART * p.hk * TC_M; i += NTHREADS) heap[i] = Num<float>::inf();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -515,17 +538,22 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   } else {
     // ---------------- epilogue: one query row per thread ----------------
     const int lq = warp & 3;            // TMEM lane quarter this warp may access
-    const int part = (warp - 2) >> 2;   // column range of the tile; part 0 owns the heap
-    const bool owner = part == 0;
+    const int part = (warp - 2) >> 2;   // column range of the tile (and heap) of this warp
     const int row = lq * 32 + lane;
     const int gq = qt * TC_M + row;
     const bool valid = gq < Qn && (!p.rowmap || p.rowmap[gq] >= 0);
+    float *const myheap = heap + part * p.hk * TC_M;
+    const float *const otherheap = heap + (NPART - 1 - part) * p.hk * TC_M;
+    const int P = NPART * p.S;  // partitions of a query
     EpiState s;
     s.cnt = 0;
     s.ovf = 0;
-    s.shared = Num<float>::inf();
+    s.o1 = Num<float>::inf();
+    s.o2 = Num<float>::inf();
+    s.pub = Num<float>::inf();
     s.n_ev = s.n_ins = s.n_it = s.n_sc = 0;
-    unsigned *ksh = p.kth_shared + (valid ? gq : 0);
+    unsigned *const pslot = p.proot + (size_t)(valid ? gq : 0) * P + NPART * split + part;
+    const unsigned *const prow = p.proot + (size_t)(valid ? gq : 0) * P;
     float pend[PEND];
     int np = 0;
 #pragma unroll
@@ -548,7 +576,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         if (mx > -Num<float>::inf()) s.thr0 = mx + s.E2;
       }
       refresh_threshold(s);
-      if (split == 0 && owner) p.margin[gq] = s.E2;
+      if (split == 0 && part == 0) p.margin[gq] = s.E2;
     } else {
       // padding row: its log and shared-bound pointers alias query 0, so it must never admit a
       // candidate; the -inf ceiling survives every threshold refresh
@@ -596,17 +624,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         if (col < p.dbg_ncols) p.dbg[(size_t)gq * p.dbg_ld + col] = __uint_as_float(r[i]) + s.qn;
       }
     };
-    // Slow part, for a chunk in which some lane has a candidate under its threshold. Every
-    // lane logs its own survivors, one predicated compare-and-store per column through
-    // compile-time register indices (no runtime selection, no loop over survivors), and the
-    // row's heap takes the chunk's minimum. The heap therefore holds the k smallest of a subset
-    // of the candidates seen (one real candidate per entry), so its root still bounds the k-th
-    // smallest approximate distance from above, and every candidate within 2E of the final
-    // k-th stays under the threshold and is logged.
     // Slow part, for a chunk in which some lane has a candidate under its threshold: a
     // warp-convergent pass in which every lane with pending candidates logs one of them per
-    // iteration (selected from its registers by index) and, for the row's owner, defers its
-    // heap insert.
+    // iteration (selected from its registers by index) and defers its heap insert.
     auto slow = [&](const uint32_t (&r)[32], size_t cbase, int c0) {
       // (a compaction that frees less than half of the log marks it overflowed: repeated
       // compactions that each free a few entries would cost a full read of the log per chunk)
@@ -644,39 +664,48 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         for (int w = 8, bit = 8; w >= 1; w >>= 1, bit >>= 1)
 #pragma unroll
           for (int j = 0; j < w; j++) t16[j] = (i & bit) ? t16[j + w] : t16[j];
-        epi_candidate(s, t16[0], (uint32_t)(cbase + c0 + i), act && valid, lg, p.logcap, owner,
-                      pend, np);
-        if (__any_sync(FULL_MASK, np == PEND)) {
-          if (owner) epi_flush(s, heap, row, p.k, pend, np, ksh);
-        }
+        epi_candidate(s, t16[0], (uint32_t)(cbase + c0 + i), act && valid, lg, p.logcap, pend,
+                      np);
+        if (__any_sync(FULL_MASK, np == PEND)) epi_flush(s, myheap, row, p.hk, pend, np, pslot);
       }
     };
-    // what the query's other splits have found (all bits set = nothing yet); the load for the
-    // next tile is issued a tile ahead so its latency hides behind the tile's work
-    unsigned sh_next = valid ? __ldcg(ksh) : 0xFFFFFFFFu;
+    // the two smallest roots up to W - 1 other splits have published (all bits set, which
+    // orders last: a heap not full yet); the loads for the next tile are issued a tile ahead
+    // so their latency hides behind the tile's work
+    auto read_window = [&](unsigned &m1, unsigned &m2) {
+      m1 = m2 = 0xFFFFFFFFu;
+      for (int w = 1; w < p.W; w++) {
+        int sp = split + w;
+        if (sp >= p.S) sp -= p.S;
+        const uint2 v = __ldcg(reinterpret_cast<const uint2 *>(prow + NPART * sp));
+        m2 = min(m2, max(m1, v.x));
+        m1 = min(m1, v.x);
+        m2 = min(m2, max(m1, v.y));
+        m1 = min(m1, v.y);
+      }
+    };
+    auto as_bound = [](unsigned u) {
+      return u == 0xFFFFFFFFu ? Num<float>::inf() : __uint_as_float(u);
+    };
+    unsigned win1 = 0xFFFFFFFFu, win2 = 0xFFFFFFFFu;
+    if (valid) read_window(win1, win2);
     const long long t_start = p.counters ? clock64() : 0;
     long long w_tfull = 0;
     for (int lt = 0; lt < ntile && !failed; lt++) {
       const int b = lt & 1, c = lt % CN_SLOTS;
       const uint32_t use = (uint32_t)(lt >> 1), cuse = (uint32_t)(lt / CN_SLOTS);
       if (valid) {
-        const float sh = __uint_as_float(sh_next);
-        bool tighter = false;
-        if (sh < s.shared) {
-          s.shared = sh;
-          tighter = true;
+        // the other part of this lane quarter (same rows, other columns) keeps its heap in
+        // shared memory: its root is read directly (one 4-byte word, written whole)
+        const float a = *reinterpret_cast<volatile const float *>(&otherheap[row]);
+        const float w1 = as_bound(win1), w2 = as_bound(win2);
+        const float o1 = fminf(a, w1), o2 = fminf(fmaxf(a, w1), w2);
+        if (o1 < s.o1 || o2 < s.o2) {
+          s.o1 = fminf(s.o1, o1);
+          s.o2 = fminf(s.o2, o2);
+          refresh_threshold(s);
         }
-        if (!owner) {
-          // the row's owner warp (same TMEM lane quarter, other half of the columns) keeps the
-          // heap: its root bounds this warp's threshold too (one 4-byte word, written whole)
-          const float ro = *reinterpret_cast<volatile const float *>(&heap[row]);
-          if (ro < s.root) {
-            s.root = ro;
-            tighter = true;
-          }
-        }
-        if (tighter) refresh_threshold(s);
-        sh_next = __ldcg(ksh);
+        read_window(win1, win2);
       }
       const long long t0 = p.counters ? clock64() : 0;
       if (!mbar_wait(&tfull[b], use & 1u)) { failed = true; break; }
@@ -739,11 +768,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         }
       }
     }
-    if (owner) epi_flush(s, heap, row, p.k, pend, np, ksh);
-    if (valid) {
-      p.kth[(size_t)lslot * p.Q + gq] = s.root;  // +inf for log-only warps
-      p.logcnt[(size_t)lslot * p.Q + gq] = s.cnt | (s.ovf ? (int)LOG_OVF : 0);
-    }
+    epi_flush(s, myheap, row, p.hk, pend, np, pslot);
+    if (valid) p.logcnt[(size_t)lslot * p.Q + gq] = s.cnt | (s.ovf ? (int)LOG_OVF : 0);
     if (p.counters) {
       atomicAdd(&p.counters[0], (unsigned long long)s.n_ev);
       atomicAdd(&p.counters[1], (unsigned long long)s.n_ins);
@@ -770,8 +796,7 @@ struct RerankParams {
   int Q, k, S, logcap, d;
   const uint2 *log;
   const int *logcnt;
-  const float *kth;
-  const unsigned *kth_shared;
+  const unsigned *proot;  // partition roots of tc_knn ([query][S]; S counts NPART per split)
   const float *margin;
   const float *Xq, *Xq2, *Xc, *Xc2;
   const int *qidx;
@@ -874,10 +899,19 @@ __global__ void __launch_bounds__(256) tc_rerank(RerankParams p) {
   if (hr < 0) return;                          // a padding row of a leaf panel
   // overflowed logs: the query goes to the next pass (a narrower format, or brute force)
   bool ovf = false;
-  float T = __uint_as_float(p.kth_shared[q]);  // NaN (all bits set) when nothing was published
-  for (int s = 0; s < p.S; s++) {
-    ovf |= (p.logcnt[(size_t)s * p.Q + q] & (int)LOG_OVF) != 0;
-    T = fminf(T, p.kth[(size_t)s * p.Q + q]);
+  for (int s = 0; s < p.S; s++) ovf |= (p.logcnt[(size_t)s * p.Q + q] & (int)LOG_OVF) != 0;
+  // the second smallest final root over the query's partitions (any two heaps hold k entries;
+  // all bits set, ordering last: a heap that never filled)
+  float T;
+  {
+    const unsigned *pr = p.proot + (size_t)q * p.S;
+    unsigned m1 = 0xFFFFFFFFu, m2 = 0xFFFFFFFFu;
+    for (int s = 0; s < p.S; s++) {
+      const unsigned u = pr[s];
+      m2 = min(m2, max(m1, u));
+      m1 = min(m1, u);
+    }
+    T = m2 == 0xFFFFFFFFu ? Num<float>::inf() : __uint_as_float(m2);
   }
   if (ovf) {
     if (lane == 0) p.fallback_list[atomicAdd(p.fallback_count, 1)] = p.dedup ? q : hr;
@@ -939,14 +973,12 @@ __global__ void __launch_bounds__(256) tc_rerank(RerankParams p) {
   auto flush = [&](int count) {
     double dist = Num<double>::inf();
     uint32_t id = NO_ID;
-    if (lane < count) {
-      id = p.cid[stg[lane]];
+    if (lane < count) id = p.cid[stg[lane]];
+    // batching form: an id already in the incoming row is not entered again, and costs no
+    // row gather
+    if (p.dedup && id_in_row<E>(id, li0)) id = NO_ID;
+    if (id != NO_ID)
       dist = exact_dist_lane(qv, p.Xc + (long long)id * p.d, p.d, (double)p.Xc2[id], qq);
-    }
-    if (p.dedup && id_in_row<E>(id, li0)) {
-      dist = Num<double>::inf();
-      id = NO_ID;
-    }
     if (p.counters && lane == 0) atomicAdd(&p.counters[6], (unsigned long long)count);
     double b1[1] = {dist};
     uint32_t i1[1] = {id};
@@ -1254,14 +1286,13 @@ static TcPlan tc_plan_base(int nq, int nc, int d, int k, int mode, int sms, bool
     const int N = Ns[ni];
     if (P.fmt == 0 && N == 256 && P.nkc > 4) continue;  // keep the TF32 A tile room
     for (int NST = 6; NST >= 2; NST--) {
-      SmemLayout L = tc_smem_layout(P.nkc, P.a_terms, P.b_terms, N, NST, k);
+      SmemLayout L = tc_smem_layout(P.nkc, P.a_terms, P.b_terms, N, NST, NPART * tc_heap_k(k));
       if (L.total <= smem_max) { best_N = N; best_NST = NST; break; }
     }
   }
   if (!best_N) return P;
   P.N = best_N;
   P.NST = best_NST;
-  P.smem = tc_smem_layout(P.nkc, P.a_terms, P.b_terms, P.N, P.NST, k).total;
   P.qtiles = (nq + TC_M - 1) / TC_M;
   P.r_pad = ((nc + 255) / 256) * 256;
   P.rtiles = P.r_pad / P.N;
@@ -1278,6 +1309,8 @@ static TcPlan tc_plan_base(int nq, int nc, int d, int k, int mode, int sms, bool
   }
   P.S = best_s;
   P.tiles_per_split = (P.rtiles + P.S - 1) / P.S;
+  P.hk = tc_heap_k(k);
+  P.smem = tc_smem_layout(P.nkc, P.a_terms, P.b_terms, P.N, P.NST, NPART * P.hk).total;
   P.logcap = std::max(8 * P.kp, 1024);
   // workspace: [prepared candidates | query side]
   P.cand_bytes = with_cand ? al256(tc_cand_bytes(nc, d, mode)) : 0;
@@ -1290,8 +1323,7 @@ static TcPlan tc_plan_base(int nq, int nc, int d, int k, int mode, int sms, bool
   // NPART logs per (query, split): one per epilogue warp of a lane quarter
   P.o_log = take((size_t)NPART * P.S * nq * P.logcap * 8);
   P.o_logcnt = take((size_t)NPART * P.S * nq * 4);
-  P.o_kth = take((size_t)NPART * P.S * nq * 4);
-  P.o_kth_shared = take((size_t)nq * 4);
+  P.o_proot = take((size_t)NPART * P.S * nq * 4);
   P.o_margin = take((size_t)nq * 4);
   P.o_fbl = take((size_t)nq * 4);
   P.o_fbc = take(16);
@@ -1390,7 +1422,8 @@ static cudaError_t tc_pass(const TcPlan &P, const TcCand &C, void *cand_pb, void
   float *qnrm = reinterpret_cast<float *>(base + P.o_qnrm);
   int *fbc = reinterpret_cast<int *>(base + P.o_fbc);
   cudaError_t e = cudaMemsetAsync(fbc, 0, 16, st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(base + P.o_kth_shared, 0xFF, (size_t)nq * 4, st);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(base + P.o_proot, 0xFF, (size_t)NPART * P.S * nq * 4, st);
   if (e != cudaSuccess) return e;
   // tracer brackets; `nk` = kernels of this file launched inside the bracket
   auto mark = [&](const char *name, bool begin, int nk = 0) {
@@ -1420,15 +1453,17 @@ static cudaError_t tc_pass(const TcPlan &P, const TcCand &C, void *cand_pb, void
   }
   TcParams tp{};
   tp.Q = nq; tp.k = k; tp.nkc = P.nkc; tp.ntiles_r = P.rtiles;
-  tp.tiles_per_split = P.tiles_per_split; tp.N = P.N; tp.NST = P.NST; tp.logcap = P.logcap;
+  tp.N = P.N; tp.NST = P.NST; tp.logcap = P.logcap;
   tp.a_terms = P.a_terms; tp.b_terms = P.b_terms; tp.fmt = P.fmt;
   tp.idesc = idesc_f32acc(P.fmt == 0 ? 2u : 1u, TC_M, P.N);
   tp.cn = C.cn; tp.cid = C.cid; tp.qn = qn; tp.qnrm = qnrm; tp.stats = C.stats;
   tp.Din = D; tp.ldD = ldD; tp.coefA = P.coefA; tp.coefB = P.coefB;
   tp.log = reinterpret_cast<uint2 *>(base + P.o_log);
   tp.logcnt = reinterpret_cast<int *>(base + P.o_logcnt);
-  tp.kth = reinterpret_cast<float *>(base + P.o_kth);
-  tp.kth_shared = reinterpret_cast<unsigned *>(base + P.o_kth_shared);
+  tp.proot = reinterpret_cast<unsigned *>(base + P.o_proot);
+  tp.hk = P.hk;
+  tp.W = tc_window(P.S);
+  tp.S = P.S;
   tp.margin = reinterpret_cast<float *>(base + P.o_margin);
   tp.status = status;
   tp.dbg = dbg;
@@ -1456,8 +1491,8 @@ static cudaError_t tc_pass(const TcPlan &P, const TcCand &C, void *cand_pb, void
 
   RerankParams rp{};
   rp.Q = nq; rp.k = k; rp.S = NPART * P.S; rp.logcap = P.logcap; rp.d = d;
-  rp.log = tp.log; rp.logcnt = tp.logcnt; rp.kth = tp.kth; rp.margin = tp.margin;
-  rp.kth_shared = tp.kth_shared;
+  rp.log = tp.log; rp.logcnt = tp.logcnt; rp.margin = tp.margin;
+  rp.proot = tp.proot;
   rp.Xq = Xq; rp.Xq2 = Xq2; rp.Xc = C.Xc; rp.Xc2 = C.Xc2; rp.qidx = qidx; rp.cid = C.cid;
   rp.D = D; rp.I = I; rp.ldD = ldD;
   rp.fallback_list = reinterpret_cast<int *>(base + P.o_fbl);
@@ -1621,8 +1656,7 @@ TcLeafPlan tc_leaf_plan(long long npts, int rows_cap, int d, int k, int sms) {
   P.o_qnrm = L.o_cnrm;
   P.o_log = take((size_t)NPART * R * P.logcap * 8);
   P.o_logcnt = take((size_t)NPART * R * 4);
-  P.o_kth = take((size_t)NPART * R * 4);
-  P.o_kth_shared = take(R * 4);
+  P.o_proot = take((size_t)NPART * R * 4);
   P.o_margin = take(R * 4);
   P.o_fbl = take(R * 4);
   P.o_fbc = take(16);
@@ -1656,7 +1690,7 @@ cudaError_t tc_leaf_pass(const TcLeafPlan &L, void *ws, const float *X, const fl
   int *fbc = reinterpret_cast<int *>(base + P.o_fbc);
   cudaError_t e = cudaMemsetAsync(stats, 0, 16, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(fbc, 0, 16, st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(base + P.o_kth_shared, 0xFF, (size_t)rows * 4, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(base + P.o_proot, 0xFF, (size_t)NPART * rows * 4, st);
   if (e != cudaSuccess) return e;
   if (setup) {
     // once per workspace: the row index map, and the shift (mean of a strided sample of the
@@ -1679,15 +1713,17 @@ cudaError_t tc_leaf_pass(const TcLeafPlan &L, void *ws, const float *X, const fl
   if (e != cudaSuccess) return e;
   TcParams tp{};
   tp.Q = rows; tp.k = k; tp.nkc = P.nkc; tp.ntiles_r = rows / P.N;
-  tp.tiles_per_split = rows / P.N; tp.N = P.N; tp.NST = P.NST; tp.logcap = P.logcap;
+  tp.N = P.N; tp.NST = P.NST; tp.logcap = P.logcap;
   tp.a_terms = P.a_terms; tp.b_terms = P.b_terms; tp.fmt = P.fmt;
   tp.idesc = idesc_f32acc(1u, TC_M, P.N);
   tp.cn = cn; tp.cid = cid; tp.qn = cn; tp.qnrm = cnrm; tp.stats = stats;
   tp.Din = D; tp.ldD = ldD; tp.coefA = P.coefA; tp.coefB = P.coefB;
   tp.log = reinterpret_cast<uint2 *>(base + P.o_log);
   tp.logcnt = reinterpret_cast<int *>(base + P.o_logcnt);
-  tp.kth = reinterpret_cast<float *>(base + P.o_kth);
-  tp.kth_shared = reinterpret_cast<unsigned *>(base + P.o_kth_shared);
+  tp.proot = reinterpret_cast<unsigned *>(base + P.o_proot);
+  tp.hk = P.hk;
+  tp.W = tc_window(P.S);
+  tp.S = P.S;
   tp.margin = reinterpret_cast<float *>(base + P.o_margin);
   tp.status = status;
   tp.rowmap = pidx;
@@ -1699,8 +1735,8 @@ cudaError_t tc_leaf_pass(const TcLeafPlan &L, void *ws, const float *X, const fl
   if (e != cudaSuccess) return e;
   RerankParams rp{};
   rp.Q = rows; rp.k = k; rp.S = NPART; rp.logcap = P.logcap; rp.d = d;
-  rp.log = tp.log; rp.logcnt = tp.logcnt; rp.kth = tp.kth; rp.margin = tp.margin;
-  rp.kth_shared = tp.kth_shared;
+  rp.log = tp.log; rp.logcnt = tp.logcnt; rp.margin = tp.margin;
+  rp.proot = tp.proot;
   rp.Xq = X; rp.Xq2 = X2; rp.Xc = X; rp.Xc2 = X2; rp.qidx = iota; rp.cid = cid;
   rp.D = D; rp.I = I; rp.ldD = ldD;
   rp.fallback_list = reinterpret_cast<int *>(base + P.o_fbl);
