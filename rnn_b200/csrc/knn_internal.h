@@ -115,6 +115,10 @@ struct TcPlan {
   int N, NST, qtiles, rtiles, q_pad, r_pad, S, tiles_per_split, logcap;
   unsigned smem;
   float coefA, coefB;
+  // norm column (the candidate norms enter through the MMA): shared memory of that form (0: it
+  // does not fit), and its error-bound coefficients (coefB is shared; coefC multiplies CN)
+  unsigned smem_fold;
+  float coefA_fold, coefC_fold, coefC;
   // query-side workspace offsets (absolute within the workspace; they start after the
   // prepared-candidate area when the plan includes it)
   size_t o_pa, o_pa_lo, o_qn, o_qnrm, o_log, o_logcnt, o_proot, o_margin, o_fbl, o_fbc;
@@ -141,6 +145,7 @@ struct TcCand {
   double *mu2;
   unsigned *stats;
   void *pb, *pb_lo;
+  void *pn;  // norm panel (the MMA's norm column), null when absent
   float *cn, *cnrm;
   uint32_t *cid;
   const float *Xc, *Xc2;
@@ -150,7 +155,7 @@ struct TcCand {
   // bounds and ids are shared with the first): efmt is a format of tc_format_of_mode, -1 when
   // absent
   int efmt;
-  void *epb, *epb_lo;
+  void *epb, *epb_lo, *epn;
 };
 
 int tc_format_of_mode(int mode);
@@ -185,7 +190,7 @@ struct TcLeafPlan {
   bool ok;
   TcPlan P;        // the split-BF16 tile plan (one split), per-query area for rows_cap rows
   int rows_cap;    // panel rows one tree may need
-  size_t o_mu, o_mu2, o_stats, o_pb, o_pb_lo, o_cn, o_cnrm, o_cid, o_iota, bytes;
+  size_t o_mu, o_mu2, o_stats, o_pb, o_pb_lo, o_pn, o_cn, o_cnrm, o_cid, o_iota, bytes;
 };
 // npts: points of the table; rows_cap: panel rows one tree may use (a multiple of 128).
 TcLeafPlan tc_leaf_plan(long long npts, int rows_cap, int d, int k, int sms);

@@ -471,8 +471,9 @@ static gsknn::TcCand escalation_as_main(const gsknn::TcCand &C, int esc_mode) {
   S.d_pad = P.d_pad;
   S.pb = C.epb;
   S.pb_lo = C.epb_lo;
+  S.pn = C.epn;
   S.efmt = -1;
-  S.epb = S.epb_lo = nullptr;
+  S.epb = S.epb_lo = S.epn = nullptr;
   return S;
 }
 

@@ -109,11 +109,47 @@ __device__ __forceinline__ uint32_t to_tf32(float x) {
   return r;
 }
 
+// Norm column of candidate row r (32 bytes, the K of one MMA): -cn/2 as the exact sum of three
+// parts in the MMA input format (BF16: 3 x 8 significant bits; TF32: 3 x 11 >= the 24 of the
+// float cn), then zeros. Against an all-ones A column the MMA adds -cn/2 to <q~, c~>, so the
+// accumulator holds w = <q~, c~> - cn/2 = -v/2. A padding row holds -inf (w = -inf, v = +inf:
+// never admitted).
+__device__ __forceinline__ void write_norm_row(int fmt, void *npanel, int r, bool real, float cn) {
+  uint4 lo4 = make_uint4(0u, 0u, 0u, 0u), hi4 = make_uint4(0u, 0u, 0u, 0u);
+  const float x = -0.5f * cn;
+  if (fmt == 0) {
+    uint32_t h = 0xFF800000u, m = 0u, l = 0u;
+    if (real) {
+      h = to_tf32(x);
+      const float r1 = x - __uint_as_float(h);
+      m = to_tf32(r1);
+      l = to_tf32(r1 - __uint_as_float(m));
+    }
+    lo4 = make_uint4(h, m, l, 0u);
+  } else {
+    uint32_t h = 0xFF80u, m = 0u, l = 0u;
+    if (real) {
+      const __nv_bfloat16 bh = __float2bfloat16_rn(x);
+      const float r1 = x - __bfloat162float(bh);
+      const __nv_bfloat16 bm = __float2bfloat16_rn(r1);
+      const __nv_bfloat16 bl = __float2bfloat16_rn(r1 - __bfloat162float(bm));
+      h = __bfloat16_as_ushort(bh);
+      m = __bfloat16_as_ushort(bm);
+      l = __bfloat16_as_ushort(bl);
+    }
+    lo4 = make_uint4(h | (m << 16), l, 0u, 0u);
+  }
+  uint4 *dst = reinterpret_cast<uint4 *>(static_cast<char *>(npanel) + (size_t)r * 32);
+  dst[0] = lo4;
+  dst[1] = hi4;
+}
+
 // fmt: 0 = TF32 (4-byte panel), 1 = BF16, 2 = split BF16 (hi and lo panels)
 // Optional forms: `dcount` (device) replaces `count` and limits the panel to the tiles it needs;
 // `rowmap` packs point idx[rowmap[r]] as row r; `gate` (device) skips all work when it reads 0;
 // a null `enorm` writes the panels only (norms, bounds, ids and statistics are left alone);
-// `pad_ok` packs index -1 as an empty padding row instead of reporting it.
+// `pad_ok` packs index -1 as an empty padding row instead of reporting it; `npanel` (candidates)
+// receives each row's norm column (write_norm_row).
 __global__ void __launch_bounds__(256) tc_pack(
     int fmt, const float *__restrict__ X, const float *__restrict__ X2, int d, int d_pad,
     long long nrows, const int *__restrict__ idx, int count, int rows_pad,
@@ -121,7 +157,7 @@ __global__ void __launch_bounds__(256) tc_pack(
     void *panel_lo, float *__restrict__ enorm, float *__restrict__ cnrm,
     uint32_t *__restrict__ ids, unsigned *__restrict__ stats, int *__restrict__ status,
     const int *__restrict__ dcount = nullptr, const int *__restrict__ rowmap = nullptr,
-    const int *__restrict__ gate = nullptr, int pad_ok = 0) {
+    const int *__restrict__ gate = nullptr, int pad_ok = 0, void *npanel = nullptr) {
   const int lane = threadIdx.x & 31;
   const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (gate && *gate == 0) return;
@@ -167,6 +203,11 @@ __global__ void __launch_bounds__(256) tc_pack(
     s2 += __shfl_xor_sync(FULL_MASK, s2, o);
     smx += __shfl_xor_sync(FULL_MASK, smx, o);
   }
+  if (lane == 0 && npanel) {
+    // the same effective norm as below (the epilogue's cn), as the MMA's norm column
+    const float enf = row >= 0 ? (float)((double)X2[row] - 2.0 * smx + *mu2) : 0.0f;
+    write_norm_row(fmt, npanel, r, row >= 0, enf);
+  }
   if (lane == 0 && enorm) {
     if (row >= 0) {
       // |x - mu|^2 expressed through the caller's norm: X2 - 2 mu.x + mu.mu
@@ -203,7 +244,7 @@ struct TcParams {
   const unsigned *stats;
   const float *Din;
   int ldD;
-  float coefA, coefB;
+  float coefA, coefB, coefC;
   uint2 *log;
   int *logcnt;
   // Partition bound. A query's candidates fall into P = NPART * S partitions (split, part). Each
@@ -235,23 +276,30 @@ struct TcParams {
 };
 
 struct SmemLayout {
-  uint32_t a_off, b_off, heap_off, cn_off, bar_off, tmem_off, total;
+  uint32_t a_off, b_off, an_off, bn_off, heap_off, cn_off, bar_off, tmem_off, total;
 };
+
+// Norm column (fold): an all-ones A tile and two slots of candidate norm tiles, 32-byte rows.
+constexpr int NORM_ROW = 32;
 
 // Partition bound (see TcParams::proot): heap entries per row and part, and the splits whose
 // published roots a row reads (its own and up to three more).
 __host__ __device__ inline int tc_heap_k(int k) { return (k + NPART - 1) / NPART; }
 __host__ __device__ inline int tc_window(int S) { return S < 4 ? S : 4; }
 
-// heap_row: heap entries per row over all epilogue parts
+// heap_row: heap entries per row over all epilogue parts; fold: the norm column areas
 __host__ __device__ inline SmemLayout tc_smem_layout(int nkc, int a_terms, int b_terms, int N,
-                                                     int NST, int heap_row) {
+                                                     int NST, int heap_row, bool fold = false) {
   SmemLayout L;
   uint32_t off = 0;
   L.a_off = off;
   off += (uint32_t)a_terms * nkc * A_CHUNK;
   L.b_off = off;
   off += (uint32_t)NST * b_terms * N * CHUNK_BYTES;
+  L.an_off = off;  // 1024-aligned: every area above is a multiple of 1 KB
+  off += fold ? (uint32_t)TC_M * NORM_ROW : 0u;
+  L.bn_off = off;
+  off += fold ? 2u * N * NORM_ROW : 0u;
   L.heap_off = off;
   off += (uint32_t)heap_row * TC_M * 4;
   off = (off + 15) & ~15u;
@@ -259,7 +307,8 @@ __host__ __device__ inline SmemLayout tc_smem_layout(int nkc, int a_terms, int b
   off += (uint32_t)CN_SLOTS * N * 4;
   off = (off + 7) & ~7u;
   L.bar_off = off;
-  off += (uint32_t)(2 * NST + 5 + CN_SLOTS) * 8;  // full, empty, tfull[2], tempty[2], afull, cnfull
+  // full, empty, tfull[2], tempty[2], afull, cnfull, nfull[2], nempty[2]
+  off += (uint32_t)(2 * NST + 9 + CN_SLOTS) * 8;
   L.tmem_off = off;
   off += 16;
   L.total = off + 1024;  // alignment slack
@@ -269,7 +318,8 @@ __host__ __device__ inline SmemLayout tc_smem_layout(int nkc, int a_terms, int b
 struct EpiState {
   // root: this part's heap root; o1 <= o2: the two smallest roots among the other partitions
   // the row reads (as last published); pub: what this part last published
-  float qn, E2, thr0, root, o1, o2, pub, thr, Tv;
+  // Tv: the filter bound on v = d' - qn'; Tw = -Tv/2 the same bound on w = -v/2 (norm column)
+  float qn, E2, thr0, root, o1, o2, pub, thr, Tv, Tw;
   int cnt;
   int ovf;
   // optional diagnostics: logged candidates, heap inserts, convergent-loop iterations, chunks
@@ -287,10 +337,12 @@ __device__ __forceinline__ void refresh_threshold(EpiState &s) {
   // query is finished by a later pass), so its chunks stop taking the slow path
   if (s.thr == -Num<float>::inf() || s.ovf) {
     s.Tv = -Num<float>::inf();
+    s.Tw = Num<float>::inf();
     return;
   }
   // filter in the v = d' - qn' space with slack for the rounding of the subtraction
   s.Tv = (s.thr - s.qn) + (fabsf(s.thr) + fabsf(s.qn)) * 2.4e-7f + 1e-30f;
+  s.Tw = -0.5f * s.Tv;  // exact: v <= Tv  <=>  w >= Tw
 }
 
 // Replace the heap root by x (< root) and sift down; returns the new root. Heap of k floats,
@@ -376,11 +428,14 @@ __device__ __forceinline__ void epi_flush(EpiState &s, float *heap, int row, int
   refresh_threshold(s);
 }
 
-template <int FMT>
+// FOLD: the candidate norms enter through the MMA (the norm column, write_norm_row), so the
+// accumulator holds w = -v/2 and the epilogue filters it directly; else the epilogue forms
+// v = cn - 2<q~, c~> from the norms it reads into shared memory.
+template <int FMT, bool FOLD>
 __global__ void __launch_bounds__(NTHREADS, 1)
     tc_knn(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tAlo,
            const __grid_constant__ CUtensorMap tB, const __grid_constant__ CUtensorMap tBlo,
-           const TcParams p) {
+           const __grid_constant__ CUtensorMap tBn, const TcParams p) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // escalation pass: launched for the largest possible query count, the tiles past the count
   // on the device exit before any set-up
@@ -391,9 +446,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   if (!p.qtab && (int)blockIdx.x * TC_M >= Qn) return;
   const uint32_t raw = su32(smem_raw);
   unsigned char *smem = smem_raw + ((1024u - (raw & 1023u)) & 1023u);
-  const SmemLayout L = tc_smem_layout(p.nkc, p.a_terms, p.b_terms, p.N, p.NST, NPART * p.hk);
+  const SmemLayout L =
+      tc_smem_layout(p.nkc, p.a_terms, p.b_terms, p.N, p.NST, NPART * p.hk, FOLD);
   unsigned char *sA = smem + L.a_off;
   unsigned char *sB = smem + L.b_off;
+  unsigned char *sAn = smem + L.an_off;
+  unsigned char *sBn = smem + L.bn_off;
   float *heap = reinterpret_cast<float *>(smem + L.heap_off);
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L.bar_off);
   uint64_t *full = bars;
@@ -402,6 +460,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   uint64_t *tempty = bars + 2 * p.NST + 2;
   uint64_t *afull = bars + 2 * p.NST + 4;
   uint64_t *cnfull = bars + 2 * p.NST + 5;
+  uint64_t *nfull = cnfull + CN_SLOTS;  // norm tile of slot b landed
+  uint64_t *nempty = nfull + 2;         // norm tile of slot b read by the tile's MMAs
   float *cn_s = reinterpret_cast<float *>(smem + L.cn_off);
   uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(smem + L.tmem_off);
 
@@ -434,6 +494,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     }
     mbar_init(afull, 1);
     for (int c = 0; c < CN_SLOTS; c++) mbar_init(&cnfull[c], 1);
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&nfull[b], 1);
+      mbar_init(&nempty[b], 1);
+    }
     mbar_fence_init();
   }
   if (warp == 1) {
@@ -443,6 +507,14 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   // the per-row heaps start at +inf before any epilogue warp reads a root (each part of a lane
   // quarter reads the other's root as part of its bound)
   for (int i = threadIdx.x; i < NPART * p.hk * TC_M; i += NTHREADS) heap[i] = Num<float>::inf();
+  if (FOLD) {
+    // the all-ones A side of the norm column (every 16-byte chunk alike, so any swizzle of it is
+    // the same bytes), made visible to the tensor core's operand reads
+    const uint32_t one = FMT == 0 ? 0x3F800000u : 0x3F803F80u;
+    uint32_t *an = reinterpret_cast<uint32_t *>(sAn);
+    for (int i = threadIdx.x; i < TC_M * NORM_ROW / 4; i += NTHREADS) an[i] = one;
+    fence_proxy_async_smem();
+  }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -462,8 +534,16 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           tma_load_2d(sA + (p.nkc + kc) * A_CHUNK, &tAlo, kc * celems, qt * TC_M, afull);
       }
       int it = 0;
+      if (FOLD) prefetch_tmap(&tBn);
       for (int lt = 0; lt < ntile && !failed; lt++) {
         const int tile = t_begin + lt;
+        if (FOLD) {
+          // the tile's norm column, into slot lt & 1 once the MMAs of tile lt - 2 read it
+          const int nb = lt & 1;
+          if (!mbar_wait(&nempty[nb], ((uint32_t)(lt >> 1) & 1u) ^ 1u)) { failed = true; break; }
+          mbar_expect_tx(&nfull[nb], (uint32_t)(N * NORM_ROW));
+          tma_load_2d(sBn + (uint32_t)nb * N * NORM_ROW, &tBn, 0, tile * N, &nfull[nb]);
+        }
         for (int kc = 0; kc < p.nkc; kc++, it++) {
           const int s = it % p.NST;
           const uint32_t round = (uint32_t)(it / p.NST);
@@ -493,11 +573,22 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         if (p.counters) w_tempty += clock64() - t0;
         // every epilogue warp has released tile lt - 2, so all of them are done with tile lt - 3
         // and its norm slot: fetch this tile's candidate norms there
-        const int c = lt % CN_SLOTS;
-        mbar_expect_tx(&cnfull[c], (uint32_t)(N * 4));
-        bulk_g2s(cn_s + c * N, p.cn + (size_t)(t_begin + lt) * N, (uint32_t)(N * 4), &cnfull[c]);
-        tc_fence_after();
         const uint32_t tmem_d = tmem_base + (uint32_t)(b * N);
+        if (FOLD) {
+          // the norm column first: w = -cn/2, then the products accumulate onto it
+          if (!mbar_wait(&nfull[b], use & 1u)) { failed = true; break; }
+          tc_fence_after();
+          const uint64_t ad = sdesc_k_sw32(su32(sAn));
+          const uint64_t bd = sdesc_k_sw32(su32(sBn) + (uint32_t)b * N * NORM_ROW);
+          if (FMT == 0) mma_tf32(tmem_d, ad, bd, p.idesc, 0u);
+          else mma_f16(tmem_d, ad, bd, p.idesc, 0u);
+        } else {
+          const int c = lt % CN_SLOTS;
+          mbar_expect_tx(&cnfull[c], (uint32_t)(N * 4));
+          bulk_g2s(cn_s + c * N, p.cn + (size_t)(t_begin + lt) * N, (uint32_t)(N * 4),
+                   &cnfull[c]);
+          tc_fence_after();
+        }
         for (int kc = 0; kc < p.nkc; kc++, it++) {
           const int s = it % p.NST;
           const uint32_t round = (uint32_t)(it / p.NST);
@@ -512,7 +603,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             const uint32_t off = (uint32_t)ks * 32u;
             const uint64_t ad = sdesc_k_sw128(a_chunk + off);
             const uint64_t bd = sdesc_k_sw128(b_chunk + off);
-            const uint32_t first = (kc == 0 && ks == 0) ? 0u : 1u;
+            const uint32_t first = (!FOLD && kc == 0 && ks == 0) ? 0u : 1u;
             if (FMT == 0) {
               mma_tf32(tmem_d, ad, bd, p.idesc, first);
             } else {
@@ -527,7 +618,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           }
           mma_commit(&empty[s]);
         }
-        if (!failed) mma_commit(&tfull[b]);
+        if (!failed) {
+          if (FOLD) mma_commit(&nempty[b]);
+          mma_commit(&tfull[b]);
+        }
       }
       if (p.counters) {
         atomicAdd(&p.counters[7], (unsigned long long)w_full);
@@ -567,7 +661,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       const float M = __uint_as_float(p.stats[0]);
       const float CN = __uint_as_float(p.stats[1]);
       const float qa = p.qnrm[gq];
-      const float E = p.coefA * qa * M + p.coefB * (CN + fabsf(s.qn) + 2.0f * qa * M);
+      const float E =
+          p.coefA * qa * M + p.coefB * (CN + fabsf(s.qn) + 2.0f * qa * M) + p.coefC * CN;
       s.E2 = 2.0f * E;
       if (p.Din) {
         float mx = -Num<float>::inf();
@@ -583,6 +678,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       s.thr0 = -Num<float>::inf();
       s.thr = -Num<float>::inf();
       s.Tv = -Num<float>::inf();
+      s.Tw = Num<float>::inf();
     }
     const int lslot = NPART * split + part;  // this warp's log among the NPART*S logs of the query
     uint2 *lg = p.log + ((size_t)lslot * p.Q + (valid ? gq : 0)) * p.logcap;
@@ -592,7 +688,20 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     // Fast part of a 32-column chunk: d' - qn' (the v space) over the accumulator values in
     // place, and their minimum (a tree of depth 5). Two chunks' fast parts run back to back in
     // one basic block so their independent arithmetic overlaps.
+    // With the norm column (FOLD) the registers already hold w = -v/2 and the fast part is the
+    // maximum alone.
     auto fast = [&](uint32_t (&r)[32], const float *cnt, int c0) -> float {
+      if constexpr (FOLD) {
+        float m11[11];
+#pragma unroll
+        for (int j = 0; j < 10; j++)
+          m11[j] = fmax3(__uint_as_float(r[3 * j]), __uint_as_float(r[3 * j + 1]),
+                         __uint_as_float(r[3 * j + 2]));
+        m11[10] = fmaxf(__uint_as_float(r[30]), __uint_as_float(r[31]));
+        const float n0 = fmax3(m11[0], m11[1], m11[2]), n1 = fmax3(m11[3], m11[4], m11[5]);
+        const float n2 = fmax3(m11[6], m11[7], m11[8]), n3 = fmaxf(m11[9], m11[10]);
+        return fmaxf(fmax3(n0, n1, n2), n3);
+      }
       const float4 *cn4 = reinterpret_cast<const float4 *>(cnt + c0);
 #pragma unroll
       for (int j = 0; j < 8; j++) {
@@ -618,10 +727,13 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       const float n2 = fmin3(m11[6], m11[7], m11[8]), n3 = fminf(m11[9], m11[10]);
       return fminf(fmin3(n0, n1, n2), n3);
     };
+    // whether a chunk's extreme value (minimum v, or maximum w with the norm column) admits
+    auto hit = [&](float m) { return FOLD ? m >= s.Tw : m <= s.Tv; };
     auto dbg_write = [&](const uint32_t (&r)[32], size_t cbase, int c0) {
       for (int i = 0; i < 32; i++) {
         const long long col = (long long)cbase + c0 + i;
-        if (col < p.dbg_ncols) p.dbg[(size_t)gq * p.dbg_ld + col] = __uint_as_float(r[i]) + s.qn;
+        const float v = FOLD ? -2.0f * __uint_as_float(r[i]) : __uint_as_float(r[i]);
+        if (col < p.dbg_ncols) p.dbg[(size_t)gq * p.dbg_ld + col] = v + s.qn;
       }
     };
     // Slow part, for a chunk in which some lane has a candidate under its threshold: a
@@ -642,9 +754,14 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       // pass mask as an OR tree (depth 5), built by every lane
       uint32_t m16[16];
 #pragma unroll
-      for (int j = 0; j < 16; j++)
-        m16[j] = (__uint_as_float(r[2 * j]) <= s.Tv ? 1u << (2 * j) : 0u) |
-                 (__uint_as_float(r[2 * j + 1]) <= s.Tv ? 1u << (2 * j + 1) : 0u);
+      for (int j = 0; j < 16; j++) {
+        if constexpr (FOLD)
+          m16[j] = (__uint_as_float(r[2 * j]) >= s.Tw ? 1u << (2 * j) : 0u) |
+                   (__uint_as_float(r[2 * j + 1]) >= s.Tw ? 1u << (2 * j + 1) : 0u);
+        else
+          m16[j] = (__uint_as_float(r[2 * j]) <= s.Tv ? 1u << (2 * j) : 0u) |
+                   (__uint_as_float(r[2 * j + 1]) <= s.Tv ? 1u << (2 * j + 1) : 0u);
+      }
 #pragma unroll
       for (int w = 8; w >= 1; w >>= 1)
 #pragma unroll
@@ -664,8 +781,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         for (int w = 8, bit = 8; w >= 1; w >>= 1, bit >>= 1)
 #pragma unroll
           for (int j = 0; j < w; j++) t16[j] = (i & bit) ? t16[j + w] : t16[j];
-        epi_candidate(s, t16[0], (uint32_t)(cbase + c0 + i), act && valid, lg, p.logcap, pend,
-                      np);
+        const float vsel = FOLD ? -2.0f * t16[0] : t16[0];
+        epi_candidate(s, vsel, (uint32_t)(cbase + c0 + i), act && valid, lg, p.logcap, pend, np);
         if (__any_sync(FULL_MASK, np == PEND)) epi_flush(s, myheap, row, p.hk, pend, np, pslot);
       }
     };
@@ -709,7 +826,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       }
       const long long t0 = p.counters ? clock64() : 0;
       if (!mbar_wait(&tfull[b], use & 1u)) { failed = true; break; }
-      if (!mbar_wait(&cnfull[c], cuse & 1u)) { failed = true; break; }
+      if (!FOLD && !mbar_wait(&cnfull[c], cuse & 1u)) { failed = true; break; }
       if (p.counters) w_tfull += clock64() - t0;
       tc_fence_after();
       const uint32_t taddr = tmem_base + ((uint32_t)(lq * 32) << 16) + (uint32_t)(b * N);
@@ -749,8 +866,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             dbg_write(ra, cbase, c0);
             dbg_write(rb, cbase, c0 + 32);
           }
-          if (__any_sync(FULL_MASK, ma <= s.Tv)) slow(ra, cbase, c0);
-          if (__any_sync(FULL_MASK, mb <= s.Tv)) slow(rb, cbase, c0 + 32);
+          if (__any_sync(FULL_MASK, hit(ma))) slow(ra, cbase, c0);
+          if (__any_sync(FULL_MASK, hit(mb))) slow(rb, cbase, c0 + 32);
         } else {
           uint32_t ra[32];
           __syncwarp();
@@ -764,7 +881,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           }
           const float ma = fast(ra, cnt, c0);
           if (p.dbg && valid) dbg_write(ra, cbase, c0);
-          if (__any_sync(FULL_MASK, ma <= s.Tv)) slow(ra, cbase, c0);
+          if (__any_sync(FULL_MASK, hit(ma))) slow(ra, cbase, c0);
         }
       }
     }
@@ -879,6 +996,18 @@ __device__ __forceinline__ void load_heap_row(const float *D, const int *I, int 
   warp_sort<double, E>(ld, li, lane);
 }
 
+// thr <- min(thr, k-th of the ascending exact list + E), rounded up: a candidate with d' above it
+// has d > that k-th and cannot enter the list.
+template <int E>
+__device__ __forceinline__ void tighten_thr(const double (&ld)[E], int k, float Eq, float &thr) {
+  double t = ld[0];
+#pragma unroll
+  for (int e2 = 0; e2 < E; e2++)
+    if (e2 == (k - 1) / 32) t = ld[e2];
+  const double dk = __shfl_sync(FULL_MASK, t, (k - 1) & 31);
+  if (dk < 1e38) thr = fminf(thr, __fadd_ru(__double2float_ru(dk), Eq));
+}
+
 // Whether `id` (NO_ID: never) is one of the ids the warp holds in `li` (E per lane).
 template <int E>
 __device__ __forceinline__ bool id_in_row(uint32_t id, const uint32_t (&li)[E]) {
@@ -889,9 +1018,14 @@ __device__ __forceinline__ bool id_in_row(uint32_t id, const uint32_t (&li)[E]) 
   return hit && id != NO_ID;
 }
 
-template <int E>
-__global__ void __launch_bounds__(256) tc_rerank(RerankParams p) {
+constexpr int RR_BAND = 128;  // band entries (d' above the approximate k-th) a warp holds back
+
+// HOLD: entries above the approximate k-th are held back and filtered against the threshold the
+// nearly final exact k-th gives (pays where the band is wide: BF16); else one pass in log order.
+template <int E, bool HOLD>
+__device__ __forceinline__ void rerank_body(const RerankParams &p) {
   __shared__ uint32_t rr_stage[8][64];
+  __shared__ uint2 rr_band[8][HOLD ? RR_BAND : 1];
   const int lane = threadIdx.x & 31;
   const int q = blockIdx.x * 8 + (threadIdx.x >> 5);
   if (q >= (p.dQ ? *p.dQ : p.Q)) return;
@@ -949,25 +1083,34 @@ __global__ void __launch_bounds__(256) tc_rerank(RerankParams p) {
     }
     T = kth;
   }
+  // A candidate in the final top-k has d' <= d_k + E <= T + 2E. Its exact distance is also at
+  // most the k-th of any k real candidates with exact distances (the incoming row and those
+  // computed so far), so d' <= that k-th + E: the threshold tightens as the exact list fills.
   float thr = T + E2;
-  {
-    float mx = -Num<float>::inf();
-    for (int j = lane; j < p.k; j += 32) mx = fmaxf(mx, p.D[(size_t)hr * p.ldD + j]);
-    for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(FULL_MASK, mx, o));
-    if (mx > -Num<float>::inf()) thr = fminf(thr, mx + E2);
-  }
+  const float Eq = 0.5f * E2;
   double ld[E];
   uint32_t li[E];
   load_heap_row<E>(p.D, p.I, p.ldD, hr, p.k, ld, li, lane);
+  if (HOLD) {
+    tighten_thr<E>(ld, p.k, Eq, thr);
+  } else {
+    // the incoming row's largest distance bounds the k-th (as the list's k-th would)
+    float mx = -Num<float>::inf();
+    for (int j = lane; j < p.k; j += 32) mx = fmaxf(mx, p.D[(size_t)hr * p.ldD + j]);
+    for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(FULL_MASK, mx, o));
+    if (mx > -Num<float>::inf() && mx < 1e38f) thr = fminf(thr, __fadd_ru(mx, Eq));
+  }
   uint32_t li0[E];  // the incoming row's ids (the batching form's duplicate check)
 #pragma unroll
   for (int e = 0; e < E; e++) li0[e] = li[e];
   const long long qrow = p.qidx[hr];
   const float *qv = p.Xq + qrow * p.d;
   const double qq = (double)p.Xq2[qrow];
-  // Pass 2: band entries are compacted into a per-warp staging list; every 32 of them each lane
-  // computes one exact distance (independent row gathers across the lanes), then the batch is
-  // sorted and merged into the exact list.
+  // Pass 2: entries under the threshold are compacted into a per-warp staging list; every 32 of
+  // them each lane computes one exact distance (independent row gathers across the lanes), then
+  // the batch is sorted and merged into the exact list. With HOLD, entries at or under T (the k
+  // smallest d') go first; those above T are held back in shared memory (as far as it holds
+  // them) and filtered afterwards against the threshold the nearly final exact k-th gives.
   uint32_t *stg = rr_stage[threadIdx.x >> 5];
   int nb = 0;
   auto flush = [&](int count) {
@@ -985,35 +1128,94 @@ __global__ void __launch_bounds__(256) tc_rerank(RerankParams p) {
     warp_sort<double, 1>(b1, i1, lane);
     warp_merge_32<double, E>(ld, li, b1[0], i1[0], lane);
   };
-  for (int s = 0; s < p.S; s++) {
-    const int cnt = p.logcnt[(size_t)s * p.Q + q];
-    const uint2 *lg = p.log + ((size_t)s * p.Q + q) * p.logcap;
-    if (p.counters && lane == 0) atomicAdd(&p.counters[5], (unsigned long long)cnt);
-    for (int base = 0; base < cnt; base += 32) {
-      const int e = base + lane;
-      uint2 ent = make_uint2(0u, NO_ID);
-      bool take = false;
-      if (e < cnt) {
-        ent = lg[e];
-        take = __uint_as_float(ent.x) <= thr;
+  if constexpr (!HOLD) {
+    for (int s = 0; s < p.S; s++) {
+      const int cnt = p.logcnt[(size_t)s * p.Q + q];
+      const uint2 *lg = p.log + ((size_t)s * p.Q + q) * p.logcap;
+      if (p.counters && lane == 0) atomicAdd(&p.counters[5], (unsigned long long)cnt);
+      for (int base = 0; base < cnt; base += 32) {
+        const int e = base + lane;
+        uint2 ent = make_uint2(0u, NO_ID);
+        bool take = false;
+        if (e < cnt) {
+          ent = lg[e];
+          take = __uint_as_float(ent.x) <= thr;
+        }
+        const unsigned m = __ballot_sync(FULL_MASK, take);
+        if (take) stg[nb + __popc(m & ((1u << lane) - 1u))] = ent.y;
+        nb += __popc(m);
+        __syncwarp();
+        if (nb >= 32) {
+          flush(32);
+          __syncwarp();
+          const uint32_t rest = lane < nb - 32 ? stg[32 + lane] : 0u;
+          __syncwarp();
+          if (lane < nb - 32) stg[lane] = rest;
+          nb -= 32;
+          __syncwarp();
+        }
       }
-      const unsigned m = __ballot_sync(FULL_MASK, take);
-      if (take) stg[nb + __popc(m & ((1u << lane) - 1u))] = ent.y;
-      nb += __popc(m);
-      __syncwarp();
-      if (nb >= 32) {
-        flush(32);
+    }
+  } else {
+    uint2 *bnd = rr_band[threadIdx.x >> 5];
+    int nbd = 0;
+    // sources in order: the NPART * S logs, then (HOLD) the held band; one flush site
+    for (int s = 0; s < p.S + (HOLD ? 1 : 0); s++) {
+      const bool from_log = s < p.S;
+      const int cnt = from_log ? p.logcnt[(size_t)s * p.Q + q] : nbd;
+      const uint2 *lg = from_log ? p.log + ((size_t)s * p.Q + q) * p.logcap : bnd;
+      if (p.counters && lane == 0 && from_log)
+        atomicAdd(&p.counters[5], (unsigned long long)cnt);
+      for (int base = 0; base < cnt; base += 32) {
+        const int e = base + lane;
+        uint2 ent = make_uint2(0u, NO_ID);
+        bool take = false, band = false;
+        if (e < cnt) {
+          ent = lg[e];
+          const float dv = __uint_as_float(ent.x);
+          take = dv <= thr;
+          band = HOLD && from_log && take && dv > T;
+        }
+        if (HOLD && from_log) {
+          const unsigned mb = __ballot_sync(FULL_MASK, band);
+          if (nbd + __popc(mb) <= RR_BAND) {
+            if (band) bnd[nbd + __popc(mb & ((1u << lane) - 1u))] = ent;
+            nbd += __popc(mb);
+            take = take && !band;
+          }
+          __syncwarp();
+        }
+        const unsigned m = __ballot_sync(FULL_MASK, take);
+        if (take) stg[nb + __popc(m & ((1u << lane) - 1u))] = ent.y;
+        nb += __popc(m);
         __syncwarp();
-        const uint32_t rest = lane < nb - 32 ? stg[32 + lane] : 0u;
-        __syncwarp();
-        if (lane < nb - 32) stg[lane] = rest;
-        nb -= 32;
-        __syncwarp();
+        if (nb >= 32) {
+          flush(32);
+          if (HOLD) tighten_thr<E>(ld, p.k, Eq, thr);
+          __syncwarp();
+          const uint32_t rest = lane < nb - 32 ? stg[32 + lane] : 0u;
+          __syncwarp();
+          if (lane < nb - 32) stg[lane] = rest;
+          nb -= 32;
+          __syncwarp();
+        }
       }
     }
   }
   if (nb > 0) flush(nb);
   write_heap_row<E>(p.D, p.I, p.ldD, hr, p.k, ld, li, lane);
+}
+
+template <int E>
+__global__ void __launch_bounds__(256) tc_rerank(RerankParams p) {
+  rerank_body<E, false>(p);
+}
+
+// The held variant is capped at 64 registers (four CTAs per SM): this latency-bound kernel loses
+// more to fewer resident warps than to a few spills.
+template <int E>
+__global__ void __launch_bounds__(256, 4) tc_rerank_hold(RerankParams p) {
+  rerank_body<E, true>(p);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1195,6 +1397,50 @@ static cudaError_t make_panel_map(CUtensorMap *m, void *base, int elem, int d_pa
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
+// Norm panel [rows][32 bytes] (write_norm_row), box of box_rows rows, 32-byte swizzle.
+static cudaError_t make_norm_map(CUtensorMap *m, void *base, int elem, int rows, int box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return cudaErrorNotSupported;
+  cuuint64_t gdim[2] = {(cuuint64_t)(NORM_ROW / elem), (cuuint64_t)rows};
+  cuuint64_t gstride[1] = {(cuuint64_t)NORM_ROW};
+  cuuint32_t box[2] = {(cuuint32_t)(NORM_ROW / elem), (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(m, elem == 4 ? CU_TENSOR_MAP_DATA_TYPE_UINT32 : CU_TENSOR_MAP_DATA_TYPE_UINT16,
+                  2, base, gdim, gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+// Launches tc_knn in the plan's format, with the norm column when `npanel` (the candidates' norm
+// panel) is given and its areas fit; sets the matching error-bound coefficients in tp.
+template <typename Grid>
+static cudaError_t launch_tc_knn(const TcPlan &P, void *npanel, int npanel_rows, Grid grid,
+                                 const CUtensorMap &mA, const CUtensorMap &mAlo,
+                                 const CUtensorMap &mB, const CUtensorMap &mBlo, TcParams &tp,
+                                 cudaStream_t st) {
+  const bool fold = npanel && P.smem_fold;
+  CUtensorMap mBn = mB;
+  if (fold) {
+    const cudaError_t e = make_norm_map(&mBn, npanel, P.elem, npanel_rows, P.N);
+    if (e != cudaSuccess) return e;
+  }
+  tp.coefA = fold ? P.coefA_fold : P.coefA;
+  tp.coefB = P.coefB;
+  tp.coefC = fold ? P.coefC_fold : P.coefC;
+  const unsigned smem = fold ? P.smem_fold : P.smem;
+  cudaError_t e = cudaSuccess;
+  auto go = [&](auto kern) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) kern<<<grid, NTHREADS, smem, st>>>(mA, mAlo, mB, mBlo, mBn, tp);
+  };
+  if (P.fmt == 0) fold ? go(tc_knn<0, true>) : go(tc_knn<0, false>);
+  else if (P.fmt == 1) fold ? go(tc_knn<1, true>) : go(tc_knn<1, false>);
+  else fold ? go(tc_knn<2, true>) : go(tc_knn<2, false>);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  return e;
+}
+
 }  // namespace tc
 
 static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -1205,7 +1451,7 @@ int tc_format_of_mode(int mode) {
 
 // Prepared-candidate area: mu, mu2, stats, panel(s), norms, norm bounds, ids.
 struct CandLayout {
-  size_t o_mu, o_mu2, o_stats, o_pb, o_pb_lo, o_cn, o_cnrm, o_cid, bytes;
+  size_t o_mu, o_mu2, o_stats, o_pb, o_pb_lo, o_pn, o_cn, o_cnrm, o_cid, bytes;
   int fmt, elem, d_pad, r_pad;
 };
 
@@ -1224,6 +1470,7 @@ static CandLayout cand_layout(int nc, int d, int mode) {
   L.o_stats = take(16);
   L.o_pb = take((size_t)L.r_pad * L.d_pad * L.elem);
   L.o_pb_lo = L.fmt == 2 ? take((size_t)L.r_pad * L.d_pad * L.elem) : 0;
+  L.o_pn = take((size_t)L.r_pad * NORM_ROW);
   L.o_cn = take((size_t)L.r_pad * 4);
   L.o_cnrm = take((size_t)L.r_pad * 4);
   L.o_cid = take((size_t)L.r_pad * 4);
@@ -1245,11 +1492,12 @@ cudaError_t tc_cand_prepare(TcCand *C, void *mem, int nc, int d, int mode, const
   C->stats = reinterpret_cast<unsigned *>(base + L.o_stats);
   C->pb = base + L.o_pb;
   C->pb_lo = L.fmt == 2 ? base + L.o_pb_lo : nullptr;
+  C->pn = base + L.o_pn;
   C->cn = reinterpret_cast<float *>(base + L.o_cn);
   C->cnrm = reinterpret_cast<float *>(base + L.o_cnrm);
   C->cid = reinterpret_cast<uint32_t *>(base + L.o_cid);
   C->Xc = Xc; C->Xc2 = Xc2; C->nrows_c = nrows_c; C->cidx = cidx;
-  C->efmt = -1; C->epb = nullptr; C->epb_lo = nullptr;
+  C->efmt = -1; C->epb = nullptr; C->epb_lo = nullptr; C->epn = nullptr;
   cudaError_t e = cudaMemsetAsync(C->stats, 0, 16, st);
   if (e != cudaSuccess) return e;
   const int nsample = std::min(nc, 4096);
@@ -1257,7 +1505,8 @@ cudaError_t tc_cand_prepare(TcCand *C, void *mem, int nc, int d, int mode, const
   tc_mu2<<<1, 32, 0, st>>>(C->mu, d, C->mu2);
   tc_pack<<<(L.r_pad + 7) / 8, 256, 0, st>>>(L.fmt, Xc, Xc2, d, L.d_pad, nrows_c, cidx, nc,
                                             L.r_pad, C->mu, C->mu2, 1, C->pb, C->pb_lo, C->cn,
-                                            C->cnrm, C->cid, C->stats, status);
+                                            C->cnrm, C->cid, C->stats, status, nullptr, nullptr,
+                                            nullptr, 0, C->pn);
   return cudaGetLastError();
 }
 
@@ -1311,6 +1560,17 @@ static TcPlan tc_plan_base(int nq, int nc, int d, int k, int mode, int sms, bool
   P.tiles_per_split = (P.rtiles + P.S - 1) / P.S;
   P.hk = tc_heap_k(k);
   P.smem = tc_smem_layout(P.nkc, P.a_terms, P.b_terms, P.N, P.NST, NPART * P.hk).total;
+  // the norm column where its areas fit beside the same tiles: in split BF16, and in BF16 from
+  // two K chunks (measured: config 2 split BF16 -4% in tc_knn, BF16 at d = 256 -1.6%, but
+  // BF16 at d = 64 +5%)
+  {
+    const uint32_t sf =
+        tc_smem_layout(P.nkc, P.a_terms, P.b_terms, P.N, P.NST, NPART * P.hk, true).total;
+    const bool wanted = P.fmt == 2 || (P.fmt == 1 && P.nkc >= 2);
+    P.smem_fold = wanted && sf <= smem_max ? sf : 0u;
+    if (const char *v = getenv("GSKNN_TC_FOLD"))
+      if (atoi(v) == 0) P.smem_fold = 0u;
+  }
   P.logcap = std::max(8 * P.kp, 1024);
   // workspace: [prepared candidates | query side]
   P.cand_bytes = with_cand ? al256(tc_cand_bytes(nc, d, mode)) : 0;
@@ -1330,25 +1590,37 @@ static TcPlan tc_plan_base(int nq, int nc, int d, int k, int mode, int sms, bool
   P.bytes = off;
   // error-bound coefficients
   const double D = (double)P.d_pad;
-  double inp, accum;
+  double inp, accum, u;
   if (P.fmt == 2) {
-    const double u = 1.0 / 256.0;
+    u = 1.0 / 256.0;
     inp = 3.2 * u * u;
     accum = 3.0 * D * std::ldexp(1.0, -23);
   } else {
-    const double u = P.fmt == 0 ? std::ldexp(1.0, -11) : std::ldexp(1.0, -8);
+    u = P.fmt == 0 ? std::ldexp(1.0, -11) : std::ldexp(1.0, -8);
     inp = 2.0 * u + u * u;
     accum = D * std::ldexp(1.0, -23) * (1 + u) * (1 + u);
   }
   P.coefA = (float)(1.25 * 2.0 * (inp + accum + std::ldexp(1.0, -22)));
   P.coefB = (float)(1.25 * 3.0 * std::ldexp(1.0, -24) + 1e-12);
+  P.coefC = 0.0f;
+  // With the norm column the accumulation also adds the three parts of -cn/2 (exact in the
+  // input format): n = (products) + 3 terms accumulate, charged as truncation on the sum of
+  // their magnitudes, |<q~, c~>| (1 + u)^2 + CN / 2; in v = -2w that is twice as much. The final
+  // d' = v + qn' rounds once, inside the coefB term.
+  {
+    const double n = (P.fmt == 2 ? 3.0 * D : D) + 3.0;
+    const double accf = n * std::ldexp(1.0, -23);
+    P.coefA_fold = (float)(1.25 * 2.0 * (inp + accf * (1 + u) * (1 + u) + std::ldexp(1.0, -22)));
+    P.coefC_fold = (float)(1.25 * (accf + std::ldexp(1.0, -24)) + 1e-12);
+  }
   P.ok = true;
   return P;
 }
 
+// panels in one format: the data panel(s), then the norm panel
 static size_t panel_bytes(int r_pad, int d_pad, int fmt) {
   const size_t one = al256((size_t)r_pad * d_pad * (fmt == 0 ? 4 : 2));
-  return fmt == 2 ? 2 * one : one;
+  return (fmt == 2 ? 2 * one : one) + al256((size_t)r_pad * tc::NORM_ROW);
 }
 
 size_t tc_cand_panel_bytes(int nc, int d, int mode) {
@@ -1410,7 +1682,7 @@ cudaError_t tc_run(const TcPlan &P, int nq, int nc, int d, int k, const float *X
 // overflowed are appended (as heap rows) to the plan's fallback list, whose count sits at
 // base + P.o_fbc.
 static cudaError_t tc_pass(const TcPlan &P, const TcCand &C, void *cand_pb, void *cand_pb_lo,
-                           int nq, int d, int k, const float *Xq, const float *Xq2,
+                           void *cand_pn, int nq, int d, int k, const float *Xq, const float *Xq2,
                            long long nrows_q, const int *qidx, const int *dQ, const int *rowmap,
                            float *D, int *I, int ldD, char *base, int *status, float *dbg,
                            long long dbg_ld, unsigned long long *counters, cudaStream_t st,
@@ -1457,7 +1729,7 @@ static cudaError_t tc_pass(const TcPlan &P, const TcCand &C, void *cand_pb, void
   tp.a_terms = P.a_terms; tp.b_terms = P.b_terms; tp.fmt = P.fmt;
   tp.idesc = idesc_f32acc(P.fmt == 0 ? 2u : 1u, TC_M, P.N);
   tp.cn = C.cn; tp.cid = C.cid; tp.qn = qn; tp.qnrm = qnrm; tp.stats = C.stats;
-  tp.Din = D; tp.ldD = ldD; tp.coefA = P.coefA; tp.coefB = P.coefB;
+  tp.Din = D; tp.ldD = ldD;
   tp.log = reinterpret_cast<uint2 *>(base + P.o_log);
   tp.logcnt = reinterpret_cast<int *>(base + P.o_logcnt);
   tp.proot = reinterpret_cast<unsigned *>(base + P.o_proot);
@@ -1475,17 +1747,7 @@ static cudaError_t tc_pass(const TcPlan &P, const TcCand &C, void *cand_pb, void
   tp.no_compact = P.esc_mode != 0;
   dim3 grid(P.qtiles, P.S);
   mark(n_knn, true);
-  if (P.fmt == 0) {
-    e = cudaFuncSetAttribute(tc_knn<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, P.smem);
-    if (e == cudaSuccess) tc_knn<0><<<grid, NTHREADS, P.smem, st>>>(mA, mAlo, mB, mBlo, tp);
-  } else if (P.fmt == 1) {
-    e = cudaFuncSetAttribute(tc_knn<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, P.smem);
-    if (e == cudaSuccess) tc_knn<1><<<grid, NTHREADS, P.smem, st>>>(mA, mAlo, mB, mBlo, tp);
-  } else {
-    e = cudaFuncSetAttribute(tc_knn<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, P.smem);
-    if (e == cudaSuccess) tc_knn<2><<<grid, NTHREADS, P.smem, st>>>(mA, mAlo, mB, mBlo, tp);
-  }
-  if (e == cudaSuccess) e = cudaGetLastError();
+  e = launch_tc_knn(P, cand_pn, P.r_pad, grid, mA, mAlo, mB, mBlo, tp, st);
   mark(n_knn, false, 1);
   if (e != cudaSuccess) return e;
 
@@ -1501,10 +1763,15 @@ static cudaError_t tc_pass(const TcPlan &P, const TcCand &C, void *cand_pb, void
   rp.dQ = dQ;
   rp.rowmap = rowmap;
   const int rb = (nq + 7) / 8;
+  // one BF16 MMA per product leaves the widest band: hold it back behind the core entries
+  // (k <= 64: larger lists would spill the held variant's registers)
+  const bool hold = P.fmt == 1 && P.kp <= 64;
   mark(n_rr, true);
   switch (P.kp) {
-    case 32: tc_rerank<1><<<rb, 256, 0, st>>>(rp); break;
-    case 64: tc_rerank<2><<<rb, 256, 0, st>>>(rp); break;
+    case 32: hold ? tc_rerank_hold<1><<<rb, 256, 0, st>>>(rp)
+                  : tc_rerank<1><<<rb, 256, 0, st>>>(rp); break;
+    case 64: hold ? tc_rerank_hold<2><<<rb, 256, 0, st>>>(rp)
+                  : tc_rerank<2><<<rb, 256, 0, st>>>(rp); break;
     case 128: tc_rerank<4><<<rb, 256, 0, st>>>(rp); break;
     case 256: tc_rerank<8><<<rb, 256, 0, st>>>(rp); break;
     default: return cudaErrorInvalidValue;
@@ -1545,7 +1812,7 @@ cudaError_t tc_run_prepared(const TcPlan &P, const TcCand &C, int nq, int d, int
   using namespace tc;
   if (C.fmt != P.fmt || C.d_pad != P.d_pad || C.r_pad != P.r_pad) return cudaErrorInvalidValue;
   char *base = static_cast<char *>(ws);
-  cudaError_t e = tc_pass(P, C, C.pb, C.pb_lo, nq, d, k, Xq, Xq2, nrows_q, qidx, nullptr,
+  cudaError_t e = tc_pass(P, C, C.pb, C.pb_lo, C.pn, nq, d, k, Xq, Xq2, nrows_q, qidx, nullptr,
                           nullptr, D, I, ldD, base, status, dbg, dbg_ld, counters, st, hook,
                           hook_ctx, false);
   if (e != cudaSuccess) return e;
@@ -1556,19 +1823,23 @@ cudaError_t tc_run_prepared(const TcPlan &P, const TcCand &C, int nq, int d, int
   const TcPlan EP = P.esc_mode ? tc_plan_base(nq, C.nc, d, k, P.esc_mode, P.sms, false,
                                               P.max_splits)
                                : TcPlan{};
-  void *epb = nullptr, *epb_lo = nullptr;
+  void *epb = nullptr, *epb_lo = nullptr, *epn = nullptr;
   if (EP.ok && C.efmt == EP.fmt) {
     epb = C.epb;
     epb_lo = C.epb_lo;
+    epn = C.epn;
   } else if (EP.ok && P.ecand_bytes) {
+    // the layout of panel_bytes: data panel(s), then the norm panel
+    const size_t one = al256((size_t)EP.r_pad * EP.d_pad * EP.elem);
     epb = base + P.o_ecand;
-    epb_lo = EP.fmt == 2 ? base + P.o_ecand + P.ecand_bytes / 2 : nullptr;
+    epb_lo = EP.fmt == 2 ? base + P.o_ecand + one : nullptr;
+    epn = base + P.o_ecand + (EP.fmt == 2 ? 2 * one : one);
     if (hook) hook(hook_ctx, "tc_escalate", true, st, 0);
     tc_pack<<<(C.r_pad + 7) / 8, 256, 0, st>>>(EP.fmt, C.Xc, C.Xc2, d, EP.d_pad, C.nrows_c,
                                               C.cidx, C.nc, C.r_pad, C.mu, C.mu2, 1, epb,
                                               epb_lo, nullptr, nullptr, nullptr, nullptr,
                                               status, nullptr, nullptr,
-                                              reinterpret_cast<int *>(base + P.o_fbc));
+                                              reinterpret_cast<int *>(base + P.o_fbc), 0, epn);
     e = cudaGetLastError();
     if (hook) hook(hook_ctx, "tc_escalate", false, st, 1);
     if (e != cudaSuccess) return e;
@@ -1580,8 +1851,9 @@ cudaError_t tc_run_prepared(const TcPlan &P, const TcCand &C, int nq, int d, int
   C2.d_pad = EP.d_pad;
   C2.pb = epb;
   C2.pb_lo = epb_lo;
+  C2.pn = epn;
   char *ebase = base + P.o_esc;
-  e = tc_pass(EP, C2, epb, epb_lo, nq, d, k, Xq, Xq2, nrows_q, qidx,
+  e = tc_pass(EP, C2, epb, epb_lo, epn, nq, d, k, Xq, Xq2, nrows_q, qidx,
               reinterpret_cast<const int *>(base + P.o_fbc),
               reinterpret_cast<const int *>(base + P.o_fbl), D, I, ldD, ebase, status, nullptr,
               0, nullptr, st, hook, hook_ctx, true);
@@ -1601,10 +1873,12 @@ cudaError_t tc_cand_prepare_escalation(TcCand *C, void *mem, int mode, int *stat
   C->efmt = L.fmt;
   C->epb = b;
   C->epb_lo = L.fmt == 2 ? b + one : nullptr;
+  C->epn = b + (L.fmt == 2 ? 2 * one : one);
   tc_pack<<<(C->r_pad + 7) / 8, 256, 0, st>>>(L.fmt, C->Xc, C->Xc2, C->d, L.d_pad, C->nrows_c,
                                              C->cidx, C->nc, C->r_pad, C->mu, C->mu2, 1,
                                              C->epb, C->epb_lo, nullptr, nullptr, nullptr,
-                                             nullptr, status, nullptr, nullptr, nullptr);
+                                             nullptr, status, nullptr, nullptr, nullptr, 0,
+                                             C->epn);
   return cudaGetLastError();
 }
 
@@ -1646,6 +1920,7 @@ TcLeafPlan tc_leaf_plan(long long npts, int rows_cap, int d, int k, int sms) {
   L.o_stats = take(16);
   L.o_pb = take(R * P.d_pad * 2);
   L.o_pb_lo = take(R * P.d_pad * 2);
+  L.o_pn = take(R * NORM_ROW);
   L.o_cn = take(R * 4);
   L.o_cnrm = take(R * 4);
   L.o_cid = take(R * 4);
@@ -1682,7 +1957,7 @@ cudaError_t tc_leaf_pass(const TcLeafPlan &L, void *ws, const float *X, const fl
   float *mu = reinterpret_cast<float *>(base + L.o_mu);
   double *mu2 = reinterpret_cast<double *>(base + L.o_mu2);
   unsigned *stats = reinterpret_cast<unsigned *>(base + L.o_stats);
-  void *pb = base + L.o_pb, *pb_lo = base + L.o_pb_lo;
+  void *pb = base + L.o_pb, *pb_lo = base + L.o_pb_lo, *pn = base + L.o_pn;
   float *cn = reinterpret_cast<float *>(base + L.o_cn);
   float *cnrm = reinterpret_cast<float *>(base + L.o_cnrm);
   uint32_t *cid = reinterpret_cast<uint32_t *>(base + L.o_cid);
@@ -1702,7 +1977,7 @@ cudaError_t tc_leaf_pass(const TcLeafPlan &L, void *ws, const float *X, const fl
   }
   tc_pack<<<(rows + 7) / 8, 256, 0, st>>>(2, X, X2, d, P.d_pad, npts, pidx, rows, rows, mu, mu2,
                                          1, pb, pb_lo, cn, cnrm, cid, stats, status, nullptr,
-                                         nullptr, nullptr, 1);
+                                         nullptr, nullptr, 1, pn);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   CUtensorMap mA, mAlo, mB, mBlo;
@@ -1717,7 +1992,7 @@ cudaError_t tc_leaf_pass(const TcLeafPlan &L, void *ws, const float *X, const fl
   tp.a_terms = P.a_terms; tp.b_terms = P.b_terms; tp.fmt = P.fmt;
   tp.idesc = idesc_f32acc(1u, TC_M, P.N);
   tp.cn = cn; tp.cid = cid; tp.qn = cn; tp.qnrm = cnrm; tp.stats = stats;
-  tp.Din = D; tp.ldD = ldD; tp.coefA = P.coefA; tp.coefB = P.coefB;
+  tp.Din = D; tp.ldD = ldD;
   tp.log = reinterpret_cast<uint2 *>(base + P.o_log);
   tp.logcnt = reinterpret_cast<int *>(base + P.o_logcnt);
   tp.proot = reinterpret_cast<unsigned *>(base + P.o_proot);
@@ -1728,10 +2003,7 @@ cudaError_t tc_leaf_pass(const TcLeafPlan &L, void *ws, const float *X, const fl
   tp.status = status;
   tp.rowmap = pidx;
   tp.qtab = qtab;
-  e = cudaFuncSetAttribute(tc_knn<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, P.smem);
-  if (e != cudaSuccess) return e;
-  tc_knn<2><<<nqt, NTHREADS, P.smem, st>>>(mA, mAlo, mB, mBlo, tp);
-  e = cudaGetLastError();
+  e = launch_tc_knn(P, pn, rows, nqt, mA, mAlo, mB, mBlo, tp, st);
   if (e != cudaSuccess) return e;
   RerankParams rp{};
   rp.Q = rows; rp.k = k; rp.S = NPART; rp.logcap = P.logcap; rp.d = d;

@@ -136,6 +136,12 @@ __device__ __forceinline__ void fma2(float &d0, float &d1, float a0, float a1, f
       : "=f"(d0), "=f"(d1)
       : "f"(a0), "f"(a1), "f"(m), "f"(c0), "f"(c1));
 }
+__device__ __forceinline__ float fmax3(float a, float b, float c) {
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+
 __device__ __forceinline__ float fmin3(float a, float b, float c) {
   float r;
   asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
@@ -195,6 +201,25 @@ __device__ __forceinline__ uint64_t sdesc_k_sw128(uint32_t saddr) {
   d |= (uint64_t)1u << 46;
   d |= (uint64_t)2u << 61;
   return d;
+}
+
+// The same for a K-major operand in the 32-byte swizzle layout (CU_TENSOR_MAP_SWIZZLE_32B): rows
+// of 32 bytes (one MMA's K: 16 BF16 or 8 TF32 elements), 8-row groups 256 bytes apart, layout
+// type 6 (SWIZZLE_32B). The tile base must be 256-byte aligned.
+__device__ __forceinline__ uint64_t sdesc_k_sw32(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1u << 16;
+  d |= (uint64_t)(256u >> 4) << 32;
+  d |= (uint64_t)1u << 46;
+  d |= (uint64_t)6u << 61;
+  return d;
+}
+
+// Make this thread's generic-proxy writes to shared memory visible to the async proxy
+// (tensor-core operand reads).
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
 }
 
 // Instruction descriptor for kind::tf32 / kind::f16 with FP32 accumulation, K-major A and B.
