@@ -486,7 +486,7 @@ def timed(L, G, prob, mode, steps, warmup, barrier=None, clocks=None):
 
 # DRAM bytes per launch of the dominant kernel, from one ncu capture of this same workload
 # (dram__bytes_read.sum + dram__bytes_write.sum; profiles/launch_list_headline_config2.md)
-TRAFFIC = {("tc_knn", "bf16x3", N_Q): 248351744 + 308929280}
+TRAFFIC = {("tc_knn", "bf16x3", N_Q): 280260352 + 315675136}
 
 
 def roofline(mode_name, prob, trace, peaks, clk):
