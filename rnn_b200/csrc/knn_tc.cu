@@ -71,12 +71,25 @@ __global__ void __launch_bounds__(1024) tc_center(const float *__restrict__ X, i
   const int p = blockIdx.x * 32 + lane;
   double s = 0.0;
   int used = 0;
-  for (int t = warp; t < nsample; t += 32) {
-    const long long i = (long long)t * count / nsample;
-    const long long row = idx[i];
-    if (row >= 0 && row < nrows) {
-      if (p < d) s += (double)X[row * d + p];
-      used++;
+  // eight sample rows per round: their index and row loads are independent and issue together;
+  // the sum keeps the sample order
+  for (int t0 = warp; t0 < nsample; t0 += 32 * 8) {
+    float v[8];
+    bool ok[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int t = t0 + 32 * u;
+      long long row = -1;
+      if (t < nsample) row = idx[(long long)t * count / nsample];
+      ok[u] = row >= 0 && row < nrows;
+      v[u] = ok[u] && p < d ? X[row * d + p] : 0.0f;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      if (ok[u]) {
+        if (p < d) s += (double)v[u];
+        used++;
+      }
     }
   }
   ps[warp][lane] = s;
@@ -159,75 +172,90 @@ __global__ void __launch_bounds__(256) tc_pack(
     const int *__restrict__ dcount = nullptr, const int *__restrict__ rowmap = nullptr,
     const int *__restrict__ gate = nullptr, int pad_ok = 0, void *npanel = nullptr) {
   const int lane = threadIdx.x & 31;
-  const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (gate && *gate == 0) return;
   if (dcount) {
     count = *dcount;
     const int used = ((count + TC_M - 1) / TC_M) * TC_M;
     if (used < rows_pad) rows_pad = used;
   }
-  if (r >= rows_pad) return;
-  long long row = -1;
-  if (r < count) {
-    row = idx[rowmap ? rowmap[r] : r];
-    if (pad_ok && row == -1) {
-      // a padding row of a leaf panel (the batching form): silently empty
-    } else if (row < 0 || row >= nrows) {
-      if (lane == 0) atomicExch(status, GSKNN_ERR_INDEX);
-      row = -1;
-    }
-  }
-  double s2 = 0.0, smx = 0.0;
-  for (int p = lane; p < d_pad; p += 32) {
-    float y = 0.0f;
-    if (row >= 0 && p < d) {
-      const float x = X[row * d + p];
-      const float m = mu[p];
-      y = x - m;
-      smx += (double)m * (double)x;
-      s2 += (double)y * (double)y;
-    }
-    const size_t o = (size_t)r * d_pad + p;
-    if (fmt == 0) {
-      reinterpret_cast<uint32_t *>(panel)[o] = to_tf32(y);
-    } else if (fmt == 1) {
-      reinterpret_cast<__nv_bfloat16 *>(panel)[o] = __float2bfloat16_rn(y);
-    } else {
-      const __nv_bfloat16 hi = __float2bfloat16_rn(y);
-      const __nv_bfloat16 lo = __float2bfloat16_rn(y - __bfloat162float(hi));
-      reinterpret_cast<__nv_bfloat16 *>(panel)[o] = hi;
-      reinterpret_cast<__nv_bfloat16 *>(panel_lo)[o] = lo;
-    }
-  }
-  for (int o = 16; o; o >>= 1) {
-    s2 += __shfl_xor_sync(FULL_MASK, s2, o);
-    smx += __shfl_xor_sync(FULL_MASK, smx, o);
-  }
-  if (lane == 0 && npanel) {
-    // the same effective norm as below (the epilogue's cn), as the MMA's norm column
-    const float enf = row >= 0 ? (float)((double)X2[row] - 2.0 * smx + *mu2) : 0.0f;
-    write_norm_row(fmt, npanel, r, row >= 0, enf);
-  }
-  if (lane == 0 && enorm) {
-    if (row >= 0) {
-      // |x - mu|^2 expressed through the caller's norm: X2 - 2 mu.x + mu.mu
-      const double en = (double)X2[row] - 2.0 * smx + *mu2;
-      const float enf = (float)en;
-      // centred norm of the stored (FP32-rounded) shift, rounded up
-      const float nrm = (float)(sqrt(s2) * (1.0 + 1e-6)) * (1.0f + 1e-6f);
-      enorm[r] = enf;
-      cnrm[r] = nrm;
-      if (ids) ids[r] = (uint32_t)row;
-      if (is_cand) {
-        atomicMax(&stats[0], __float_as_uint(nrm));
-        atomicMax(&stats[1], __float_as_uint(fabsf(enf) * (1.0f + 1e-6f)));
+  // one row per warp, grid-stride; the candidate bound statistics are kept per warp and reach
+  // the global maxima once per warp (not once per row: same-address atomics serialize)
+  unsigned mx_nrm = 0u, mx_en = 0u;
+  const int wstride = gridDim.x * (blockDim.x >> 5);
+  for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < rows_pad;
+       r += wstride) {
+    long long row = -1;
+    if (r < count) {
+      row = idx[rowmap ? rowmap[r] : r];
+      if (pad_ok && row == -1) {
+        // a padding row of a leaf panel (the batching form): silently empty
+      } else if (row < 0 || row >= nrows) {
+        if (lane == 0) atomicExch(status, GSKNN_ERR_INDEX);
+        row = -1;
       }
-    } else {
-      enorm[r] = Num<float>::nan();
-      cnrm[r] = 0.0f;
-      if (ids) ids[r] = NO_ID;
+    }
+    double s2 = 0.0, smx = 0.0;
+    for (int p = lane; p < d_pad; p += 32) {
+      float y = 0.0f;
+      if (row >= 0 && p < d) {
+        const float x = X[row * d + p];
+        const float m = mu[p];
+        y = x - m;
+        smx += (double)m * (double)x;
+        s2 += (double)y * (double)y;
+      }
+      const size_t o = (size_t)r * d_pad + p;
+      if (fmt == 0) {
+        reinterpret_cast<uint32_t *>(panel)[o] = to_tf32(y);
+      } else if (fmt == 1) {
+        reinterpret_cast<__nv_bfloat16 *>(panel)[o] = __float2bfloat16_rn(y);
+      } else {
+        const __nv_bfloat16 hi = __float2bfloat16_rn(y);
+        const __nv_bfloat16 lo = __float2bfloat16_rn(y - __bfloat162float(hi));
+        reinterpret_cast<__nv_bfloat16 *>(panel)[o] = hi;
+        reinterpret_cast<__nv_bfloat16 *>(panel_lo)[o] = lo;
+      }
+    }
+    for (int o = 16; o; o >>= 1) {
+      s2 += __shfl_xor_sync(FULL_MASK, s2, o);
+      smx += __shfl_xor_sync(FULL_MASK, smx, o);
+    }
+    if (lane == 0 && npanel) {
+      // the same effective norm as below (the epilogue's cn), as the MMA's norm column
+      const float enf = row >= 0 ? (float)((double)X2[row] - 2.0 * smx + *mu2) : 0.0f;
+      write_norm_row(fmt, npanel, r, row >= 0, enf);
+    }
+    if (lane == 0 && enorm) {
+      if (row >= 0) {
+        // |x - mu|^2 expressed through the caller's norm: X2 - 2 mu.x + mu.mu
+        const double en = (double)X2[row] - 2.0 * smx + *mu2;
+        const float enf = (float)en;
+        // centred norm of the stored (FP32-rounded) shift, rounded up
+        const float nrm = (float)(sqrt(s2) * (1.0 + 1e-6)) * (1.0f + 1e-6f);
+        enorm[r] = enf;
+        cnrm[r] = nrm;
+        if (ids) ids[r] = (uint32_t)row;
+        // non-negative floats order like their bit patterns
+        mx_nrm = max(mx_nrm, __float_as_uint(nrm));
+        mx_en = max(mx_en, __float_as_uint(fabsf(enf) * (1.0f + 1e-6f)));
+      } else {
+        enorm[r] = Num<float>::nan();
+        cnrm[r] = 0.0f;
+        if (ids) ids[r] = NO_ID;
+      }
     }
   }
+  if (lane == 0 && enorm && is_cand && (mx_nrm | mx_en)) {
+    atomicMax(&stats[0], mx_nrm);
+    atomicMax(&stats[1], mx_en);
+  }
+}
+
+// Blocks of a tc_pack launch over `rows` panel rows: one warp per row up to 16 CTAs of 8 warps
+// per SM, grid-stride beyond.
+static inline unsigned tc_pack_grid(long long rows) {
+  const long long want = (rows + 7) / 8;
+  return (unsigned)std::max(1LL, std::min(want, 148LL * 16));
 }
 
 // ------------------------------------------------------------------------------------------
@@ -938,7 +966,8 @@ struct RerankParams {
 __device__ __forceinline__ double exact_dist_lane(const float *q, const float *c, int d,
                                                   double cc, double qq) {
   double acc = 0.0;
-  if ((d & 3) == 0 && ((reinterpret_cast<uintptr_t>(q) | reinterpret_cast<uintptr_t>(c)) & 15) == 0) {
+  const uintptr_t qc = reinterpret_cast<uintptr_t>(q) | reinterpret_cast<uintptr_t>(c);
+  if ((d & 3) == 0 && (qc & 15) == 0) {
     const float4 *q4 = reinterpret_cast<const float4 *>(q);
     const float4 *c4 = reinterpret_cast<const float4 *>(c);
     for (int i = 0; i < (d >> 2); i++) {
@@ -1503,7 +1532,7 @@ cudaError_t tc_cand_prepare(TcCand *C, void *mem, int nc, int d, int mode, const
   const int nsample = std::min(nc, 4096);
   tc_center<<<(d + 31) / 32, 1024, 0, st>>>(Xc, d, nrows_c, cidx, nc, nsample, C->mu);
   tc_mu2<<<1, 32, 0, st>>>(C->mu, d, C->mu2);
-  tc_pack<<<(L.r_pad + 7) / 8, 256, 0, st>>>(L.fmt, Xc, Xc2, d, L.d_pad, nrows_c, cidx, nc,
+  tc_pack<<<tc_pack_grid(L.r_pad), 256, 0, st>>>(L.fmt, Xc, Xc2, d, L.d_pad, nrows_c, cidx, nc,
                                             L.r_pad, C->mu, C->mu2, 1, C->pb, C->pb_lo, C->cn,
                                             C->cnrm, C->cid, C->stats, status, nullptr, nullptr,
                                             nullptr, 0, C->pn);
@@ -1705,7 +1734,7 @@ static cudaError_t tc_pass(const TcPlan &P, const TcCand &C, void *cand_pb, void
   const char *n_knn = escalation ? "tc_escalate" : "tc_knn";
   const char *n_rr = escalation ? "tc_escalate" : "tc_rerank";
   mark(n_pack, true);
-  tc_pack<<<(P.q_pad + 7) / 8, 256, 0, st>>>(P.fmt, Xq, Xq2, d, P.d_pad, nrows_q, qidx, nq,
+  tc_pack<<<tc_pack_grid(P.q_pad), 256, 0, st>>>(P.fmt, Xq, Xq2, d, P.d_pad, nrows_q, qidx, nq,
                                             P.q_pad, C.mu, C.mu2, 0, pa, pa_lo, qn, qnrm,
                                             nullptr, C.stats, status, dQ, rowmap, nullptr);
   e = cudaGetLastError();
@@ -1835,7 +1864,7 @@ cudaError_t tc_run_prepared(const TcPlan &P, const TcCand &C, int nq, int d, int
     epb_lo = EP.fmt == 2 ? base + P.o_ecand + one : nullptr;
     epn = base + P.o_ecand + (EP.fmt == 2 ? 2 * one : one);
     if (hook) hook(hook_ctx, "tc_escalate", true, st, 0);
-    tc_pack<<<(C.r_pad + 7) / 8, 256, 0, st>>>(EP.fmt, C.Xc, C.Xc2, d, EP.d_pad, C.nrows_c,
+    tc_pack<<<tc_pack_grid(C.r_pad), 256, 0, st>>>(EP.fmt, C.Xc, C.Xc2, d, EP.d_pad, C.nrows_c,
                                               C.cidx, C.nc, C.r_pad, C.mu, C.mu2, 1, epb,
                                               epb_lo, nullptr, nullptr, nullptr, nullptr,
                                               status, nullptr, nullptr,
@@ -1874,8 +1903,8 @@ cudaError_t tc_cand_prepare_escalation(TcCand *C, void *mem, int mode, int *stat
   C->epb = b;
   C->epb_lo = L.fmt == 2 ? b + one : nullptr;
   C->epn = b + (L.fmt == 2 ? 2 * one : one);
-  tc_pack<<<(C->r_pad + 7) / 8, 256, 0, st>>>(L.fmt, C->Xc, C->Xc2, C->d, L.d_pad, C->nrows_c,
-                                             C->cidx, C->nc, C->r_pad, C->mu, C->mu2, 1,
+  tc_pack<<<tc_pack_grid(C->r_pad), 256, 0, st>>>(L.fmt, C->Xc, C->Xc2, C->d, L.d_pad,
+                                             C->nrows_c, C->cidx, C->nc, C->r_pad, C->mu, C->mu2, 1,
                                              C->epb, C->epb_lo, nullptr, nullptr, nullptr,
                                              nullptr, status, nullptr, nullptr, nullptr, 0,
                                              C->epn);
@@ -1975,7 +2004,7 @@ cudaError_t tc_leaf_pass(const TcLeafPlan &L, void *ws, const float *X, const fl
                                               mu);
     tc_mu2<<<1, 32, 0, st>>>(mu, d, mu2);
   }
-  tc_pack<<<(rows + 7) / 8, 256, 0, st>>>(2, X, X2, d, P.d_pad, npts, pidx, rows, rows, mu, mu2,
+  tc_pack<<<tc_pack_grid(rows), 256, 0, st>>>(2, X, X2, d, P.d_pad, npts, pidx, rows, rows, mu, mu2,
                                          1, pb, pb_lo, cn, cnrm, cid, stats, status, nullptr,
                                          nullptr, nullptr, 1, pn);
   e = cudaGetLastError();
@@ -2021,10 +2050,22 @@ cudaError_t tc_leaf_pass(const TcLeafPlan &L, void *ws, const float *X, const fl
   fp.count = fbc;
   const int rb = (rows + 7) / 8;
   switch (P.kp) {
-    case 32: tc_rerank<1><<<rb, 256, 0, st>>>(rp); tc_fallback_leaf<1><<<148, 256, 0, st>>>(fp); break;
-    case 64: tc_rerank<2><<<rb, 256, 0, st>>>(rp); tc_fallback_leaf<2><<<148, 256, 0, st>>>(fp); break;
-    case 128: tc_rerank<4><<<rb, 256, 0, st>>>(rp); tc_fallback_leaf<4><<<148, 256, 0, st>>>(fp); break;
-    case 256: tc_rerank<8><<<rb, 256, 0, st>>>(rp); tc_fallback_leaf<8><<<148, 256, 0, st>>>(fp); break;
+    case 32:
+      tc_rerank<1><<<rb, 256, 0, st>>>(rp);
+      tc_fallback_leaf<1><<<148, 256, 0, st>>>(fp);
+      break;
+    case 64:
+      tc_rerank<2><<<rb, 256, 0, st>>>(rp);
+      tc_fallback_leaf<2><<<148, 256, 0, st>>>(fp);
+      break;
+    case 128:
+      tc_rerank<4><<<rb, 256, 0, st>>>(rp);
+      tc_fallback_leaf<4><<<148, 256, 0, st>>>(fp);
+      break;
+    case 256:
+      tc_rerank<8><<<rb, 256, 0, st>>>(rp);
+      tc_fallback_leaf<8><<<148, 256, 0, st>>>(fp);
+      break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
