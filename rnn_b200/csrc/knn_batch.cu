@@ -27,6 +27,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -378,6 +379,10 @@ struct BatchJob {
   int tc_tile;                  // candidate tile width of the panels (0: not available)
   TcLeafPlan tcl;               // plan of the allocated workspace (tcl.ok: allocated)
   void *tc_ws;
+  // GSKNN_TC_COUNTERS=1: the leaf passes' epilogue and re-rank counters (device, 16 words),
+  // printed and reset at each sync, with the panel rows and query-tile CTAs they cover
+  unsigned long long *tc_counters;
+  long long tc_cnt_rows, tc_cnt_ctas;
   int *tc_pidx;                 // device: every tree's panel rows (point or -1)
   int4 *tc_qtab;                // device: every tree's query-tile table
   int2 *tc_rtab;                // device: candidate tile range of every panel query tile
@@ -550,6 +555,8 @@ static int build_tc_plan(BatchJob *b, const int *leaf_ptr, const int *leaf_pts,
 
 static void free_tc(BatchJob *b) {
   if (b->tc_ws) cudaFree(b->tc_ws);
+  if (b->tc_counters) cudaFree(b->tc_counters);
+  b->tc_counters = nullptr;
   if (b->tc_pidx) cudaFree(b->tc_pidx);
   if (b->h_tc_pidx) cudaFreeHost(b->h_tc_pidx);
   if (b->h_tc_qtab) cudaFreeHost(b->h_tc_qtab);
@@ -609,14 +616,21 @@ static int enqueue_tc_pass(BatchJob *b, float *D, int *I) {
   BCU(cudaMemcpyAsync(b->tc_rtab, b->h_tc_rtab, (size_t)(prow / 128) * sizeof(int2),
                       cudaMemcpyHostToDevice, b->st));
   BCU(cudaEventRecord(b->staged, b->st));
+  static const bool want_counters = std::getenv("GSKNN_TC_COUNTERS") != nullptr;
+  if (want_counters && !b->tc_counters) {
+    BCU(cudaMalloc(&b->tc_counters, 16 * sizeof(unsigned long long)));
+    BCU(cudaMemsetAsync(b->tc_counters, 0, 16 * sizeof(unsigned long long), b->st));
+  }
   for (int t = 0; t < b->T; t++) {
     const long long *tr = b->h_tc_tree + 6 * t;
     if (tr[1] == 0) continue;
     BCU(gsknn::tc_leaf_pass(b->tcl, b->tc_ws, b->X, b->X2, b->N, b->d, b->k,
                             b->tc_pidx + tr[2], (int)tr[0], b->tc_qtab + tr[3], (int)tr[1],
                             b->tc_rtab + tr[4], D, I, b->ldD, b->status, b->st,
-                            !b->tc_setup_done));
+                            !b->tc_setup_done, b->tc_counters));
     b->tc_setup_done = true;
+    b->tc_cnt_rows += tr[0];
+    b->tc_cnt_ctas += tr[1];
   }
   return GSKNN_OK;
 }
@@ -899,6 +913,19 @@ int gsknn_batch_sync(gsknn_batch_t *job) {
   BatchJob *b = reinterpret_cast<BatchJob *>(job);
   if (!b) return set_err(GSKNN_ERR_ARG, "gsknn_batch_sync: null job");
   BCU(cudaStreamSynchronize(b->st));
+  if (b->tc_counters && b->tc_cnt_rows > 0) {
+    unsigned long long h[16] = {};
+    BCU(cudaMemcpy(h, b->tc_counters, sizeof(h), cudaMemcpyDeviceToHost));
+    BCU(cudaMemset(b->tc_counters, 0, sizeof(h)));
+    const double rows = (double)b->tc_cnt_rows, warps = (double)b->tc_cnt_ctas * 8;
+    std::fprintf(stderr,
+                 "gsknn batch tc: panel rows=%lld logged/row=%.1f inserts/row=%.1f "
+                 "slow-chunks/warp=%.1f chunks/warp=%.1f rerank-scanned/row=%.1f "
+                 "exact/row=%.1f\n",
+                 b->tc_cnt_rows, (double)h[0] / rows, (double)h[1] / rows, (double)h[3] / warps,
+                 (double)h[4] / warps, (double)h[5] / rows, (double)h[6] / rows);
+    b->tc_cnt_rows = b->tc_cnt_ctas = 0;
+  }
   int st = 0;
   BCU(cudaMemcpy(&st, b->status, sizeof(int), cudaMemcpyDeviceToHost));
   if (st == GSKNN_ERR_INDEX)

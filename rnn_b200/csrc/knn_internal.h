@@ -201,7 +201,8 @@ int tc_leaf_tile(int d, int k, int sms);
 cudaError_t tc_leaf_pass(const TcLeafPlan &L, void *ws, const float *X, const float *X2,
                          long long npts, int d, int k, const int *pidx, int rows,
                          const int4 *qtab, int nqt, const int2 *rtab, float *D, int *I,
-                         int ldD, int *status, cudaStream_t st, bool setup);
+                         int ldD, int *status, cudaStream_t st, bool setup,
+                         unsigned long long *counters = nullptr);
 
 cudaError_t tc_run_prepared(const TcPlan &P, const TcCand &C, int nq, int d, int k,
                             const float *Xq, const float *Xq2, long long nrows_q,

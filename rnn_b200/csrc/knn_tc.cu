@@ -1977,7 +1977,8 @@ int tc_leaf_tile(const TcLeafPlan &L) { return L.P.N; }
 cudaError_t tc_leaf_pass(const TcLeafPlan &L, void *ws, const float *X, const float *X2,
                          long long npts, int d, int k, const int *pidx, int rows,
                          const int4 *qtab, int nqt, const int2 *rtab, float *D, int *I,
-                         int ldD, int *status, cudaStream_t st, bool setup) {
+                         int ldD, int *status, cudaStream_t st, bool setup,
+                         unsigned long long *counters) {
   using namespace tc;
   const TcPlan &P = L.P;
   if (!L.ok || rows > L.rows_cap || rows % P.N != 0 || k > 256) return cudaErrorInvalidValue;
@@ -2032,6 +2033,7 @@ cudaError_t tc_leaf_pass(const TcLeafPlan &L, void *ws, const float *X, const fl
   tp.status = status;
   tp.rowmap = pidx;
   tp.qtab = qtab;
+  tp.counters = counters;
   e = launch_tc_knn(P, pn, rows, nqt, mA, mAlo, mB, mBlo, tp, st);
   if (e != cudaSuccess) return e;
   RerankParams rp{};
@@ -2044,6 +2046,7 @@ cudaError_t tc_leaf_pass(const TcLeafPlan &L, void *ws, const float *X, const fl
   rp.fallback_count = fbc;
   rp.rowmap = pidx;
   rp.dedup = 1;
+  rp.counters = counters;
   LeafFallbackParams fp{};
   fp.k = k; fp.d = d; fp.N = P.N; fp.X = X; fp.X2 = X2; fp.rowmap = pidx; fp.ids = cid;
   fp.rtab = rtab; fp.D = D; fp.I = I; fp.ldD = ldD; fp.list = rp.fallback_list;
