@@ -1084,8 +1084,12 @@ __device__ __forceinline__ void rerank_body(const RerankParams &p) {
   // Pass 1: the exact k-th smallest approximate distance over all of the query's logs. Every
   // candidate among the k smallest approximate distances was logged (its d' was below every
   // threshold in force), so this is the global approximate k-th, usually far below the bound T
-  // the splits ended with.
-  {
+  // the splits ended with. When all the logs together hold at most 32 entries (short lists:
+  // leaves of the batching form), pass 2 takes them in one batch of exact distances whatever
+  // the bound, so pass 1 is skipped and T stays the partition bound.
+  int total = 0;
+  for (int s = 0; s < p.S; s++) total += p.logcnt[(size_t)s * p.Q + q];
+  if (total > 32) {
     float kd[E];
     uint32_t ki[E];
 #pragma unroll
