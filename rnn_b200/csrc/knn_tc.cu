@@ -1008,9 +1008,11 @@ __device__ __forceinline__ void write_heap_row(float *D, int *I, int ldD, int q,
   }
 }
 
+// (sort = false leaves the list in the row's own order; sort it before merging into it)
 template <int E>
 __device__ __forceinline__ void load_heap_row(const float *D, const int *I, int ldD, int q, int k,
-                                              double (&ld)[E], uint32_t (&li)[E], int lane) {
+                                              double (&ld)[E], uint32_t (&li)[E], int lane,
+                                              bool sort = true) {
 #pragma unroll
   for (int e = 0; e < E; e++) {
     const int t = e * 32 + lane;
@@ -1022,7 +1024,7 @@ __device__ __forceinline__ void load_heap_row(const float *D, const int *I, int 
       li[e] = NO_ID;
     }
   }
-  warp_sort<double, E>(ld, li, lane);
+  if (sort) warp_sort<double, E>(ld, li, lane);
 }
 
 // thr <- min(thr, k-th of the ascending exact list + E), rounded up: a candidate with d' above it
@@ -1051,7 +1053,9 @@ constexpr int RR_BAND = 128;  // band entries (d' above the approximate k-th) a 
 
 // HOLD: entries above the approximate k-th are held back and filtered against the threshold the
 // nearly final exact k-th gives (pays where the band is wide: BF16); else one pass in log order.
-template <int E, bool HOLD>
+// LAZY (the batching form's leaf pass): the incoming row stays unsorted until a candidate can
+// enter it, and a row nothing entered is not written back.
+template <int E, bool HOLD, bool LAZY>
 __device__ __forceinline__ void rerank_body(const RerankParams &p) {
   __shared__ uint32_t rr_stage[8][64];
   __shared__ uint2 rr_band[8][HOLD ? RR_BAND : 1];
@@ -1123,7 +1127,12 @@ __device__ __forceinline__ void rerank_body(const RerankParams &p) {
   const float Eq = 0.5f * E2;
   double ld[E];
   uint32_t li[E];
-  load_heap_row<E>(p.D, p.I, p.ldD, hr, p.k, ld, li, lane);
+  // LAZY: the incoming row stays unsorted until some candidate can enter it: a batch whose
+  // exact distances all exceed the list's k-th (the row's largest distance, until the first
+  // merge) changes nothing, and a row nothing entered is not written back.
+  load_heap_row<E>(p.D, p.I, p.ldD, hr, p.k, ld, li, lane, !LAZY);
+  bool sorted = !LAZY;
+  double lim = Num<double>::inf();
   if (HOLD) {
     tighten_thr<E>(ld, p.k, Eq, thr);
   } else {
@@ -1132,6 +1141,7 @@ __device__ __forceinline__ void rerank_body(const RerankParams &p) {
     for (int j = lane; j < p.k; j += 32) mx = fmaxf(mx, p.D[(size_t)hr * p.ldD + j]);
     for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(FULL_MASK, mx, o));
     if (mx > -Num<float>::inf() && mx < 1e38f) thr = fminf(thr, __fadd_ru(mx, Eq));
+    lim = (double)mx;
   }
   uint32_t li0[E];  // the incoming row's ids (the batching form's duplicate check)
 #pragma unroll
@@ -1156,10 +1166,25 @@ __device__ __forceinline__ void rerank_body(const RerankParams &p) {
     if (id != NO_ID)
       dist = exact_dist_lane(qv, p.Xc + (long long)id * p.d, p.d, (double)p.Xc2[id], qq);
     if (p.counters && lane == 0) atomicAdd(&p.counters[6], (unsigned long long)count);
+    if (LAZY) {
+      // nothing in this batch can enter (ties are settled by the merge itself)
+      if (!__any_sync(FULL_MASK, id != NO_ID && dist <= lim)) return;
+      if (!sorted) {
+        warp_sort<double, E>(ld, li, lane);
+        sorted = true;
+      }
+    }
     double b1[1] = {dist};
     uint32_t i1[1] = {id};
     warp_sort<double, 1>(b1, i1, lane);
     warp_merge_32<double, E>(ld, li, b1[0], i1[0], lane);
+    if (LAZY) {
+      double t = ld[0];
+#pragma unroll
+      for (int e2 = 0; e2 < E; e2++)
+        if (e2 == (p.k - 1) / 32) t = ld[e2];
+      lim = __shfl_sync(FULL_MASK, t, (p.k - 1) & 31);
+    }
   };
   if constexpr (!HOLD) {
     for (int s = 0; s < p.S; s++) {
@@ -1236,19 +1261,24 @@ __device__ __forceinline__ void rerank_body(const RerankParams &p) {
     }
   }
   if (nb > 0) flush(nb);
-  write_heap_row<E>(p.D, p.I, p.ldD, hr, p.k, ld, li, lane);
+  if (sorted) write_heap_row<E>(p.D, p.I, p.ldD, hr, p.k, ld, li, lane);
 }
 
 template <int E>
 __global__ void __launch_bounds__(256) tc_rerank(RerankParams p) {
-  rerank_body<E, false>(p);
+  rerank_body<E, false, false>(p);
+}
+
+template <int E>
+__global__ void __launch_bounds__(256) tc_rerank_leaf(RerankParams p) {
+  rerank_body<E, false, true>(p);
 }
 
 // The held variant is capped at 64 registers (four CTAs per SM): this latency-bound kernel loses
 // more to fewer resident warps than to a few spills.
 template <int E>
 __global__ void __launch_bounds__(256, 4) tc_rerank_hold(RerankParams p) {
-  rerank_body<E, true>(p);
+  rerank_body<E, true, false>(p);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -2058,19 +2088,19 @@ cudaError_t tc_leaf_pass(const TcLeafPlan &L, void *ws, const float *X, const fl
   const int rb = (rows + 7) / 8;
   switch (P.kp) {
     case 32:
-      tc_rerank<1><<<rb, 256, 0, st>>>(rp);
+      tc_rerank_leaf<1><<<rb, 256, 0, st>>>(rp);
       tc_fallback_leaf<1><<<148, 256, 0, st>>>(fp);
       break;
     case 64:
-      tc_rerank<2><<<rb, 256, 0, st>>>(rp);
+      tc_rerank_leaf<2><<<rb, 256, 0, st>>>(rp);
       tc_fallback_leaf<2><<<148, 256, 0, st>>>(fp);
       break;
     case 128:
-      tc_rerank<4><<<rb, 256, 0, st>>>(rp);
+      tc_rerank_leaf<4><<<rb, 256, 0, st>>>(rp);
       tc_fallback_leaf<4><<<148, 256, 0, st>>>(fp);
       break;
     case 256:
-      tc_rerank<8><<<rb, 256, 0, st>>>(rp);
+      tc_rerank_leaf<8><<<rb, 256, 0, st>>>(rp);
       tc_fallback_leaf<8><<<148, 256, 0, st>>>(fp);
       break;
     default: return cudaErrorInvalidValue;
