@@ -24,6 +24,10 @@
 #include <thread>
 #include <vector>
 
+#if defined(__x86_64__)
+#include <emmintrin.h>
+#endif
+
 namespace gsknn {
 
 // ------------------------------------------------------------------------------------------
@@ -216,15 +220,36 @@ static cudaError_t gather_rows_to_device(const T *Xq, const T *Xq2, const int *q
   const int nch = n * row_bytes >= ((size_t)32 << 20) ? 8 : 1;
   std::unique_ptr<std::atomic<unsigned>[]> done(new std::atomic<unsigned>[nch]);
   for (int j = 0; j < nch; j++) done[j].store(0);
+#if defined(__x86_64__)
+  // The staging rows are written once and then read only by the DMA engine: non-temporal
+  // stores skip the read-for-ownership of every destination line (a third of the host memory
+  // traffic of this copy). Used when rows and the staging base are 16-byte aligned.
+  const bool stream = row_bytes % 16 == 0 && (reinterpret_cast<uintptr_t>(hrows) & 15) == 0;
+#endif
   auto part = [&](unsigned w, int j) {
     const size_t c0 = n * j / nch, c1 = n * (j + 1) / nch;
     const size_t a = c0 + (c1 - c0) * w / nt, b = c0 + (c1 - c0) * (w + 1) / nt;
     for (size_t i = a; i < b; i++) {
       const bool q = i < (size_t)nq;
       const size_t r = q ? (size_t)qidx[i] : (size_t)cidx[i - nq];
-      std::memcpy(hrows + i * d, (q ? Xq : Xc) + r * d, row_bytes);
+      const T *src = (q ? Xq : Xc) + r * d;
+#if defined(__x86_64__)
+      if (stream) {
+        const __m128i *s4 = reinterpret_cast<const __m128i *>(src);
+        __m128i *d4 = reinterpret_cast<__m128i *>(hrows + i * d);
+        for (size_t v = 0; v < row_bytes / 16; v++)
+          _mm_stream_si128(d4 + v, _mm_loadu_si128(s4 + v));
+      } else {
+        std::memcpy(hrows + i * d, src, row_bytes);
+      }
+#else
+      std::memcpy(hrows + i * d, src, row_bytes);
+#endif
       hn[i] = (q ? Xq2 : Xc2)[r];
     }
+#if defined(__x86_64__)
+    _mm_sfence();  // the streamed rows are visible before the chunk is handed to the DMA
+#endif
     done[j].fetch_add(1, std::memory_order_release);
   };
   std::vector<std::thread> pool;
