@@ -190,7 +190,7 @@ struct TcLeafPlan {
   bool ok;
   TcPlan P;        // the split-BF16 tile plan (one split), per-query area for rows_cap rows
   int rows_cap;    // panel rows one tree may need
-  size_t o_mu, o_mu2, o_stats, o_pb, o_pb_lo, o_pn, o_cn, o_cnrm, o_cid, o_iota, bytes;
+  size_t o_mu, o_mu2, o_cpart, o_stats, o_pb, o_pb_lo, o_pn, o_cn, o_cnrm, o_cid, o_iota, bytes;
 };
 // npts: points of the table; rows_cap: panel rows one tree may use (a multiple of 128).
 TcLeafPlan tc_leaf_plan(long long npts, int rows_cap, int d, int k, int sms);

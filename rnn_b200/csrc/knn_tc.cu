@@ -5,7 +5,8 @@
 // the lower id) of the caller's float inputs, merged into the caller's heaps.
 //
 // Kernels (one call):
-//   tc_center     shift vector mu = mean of a strided sample of candidate rows
+//   tc_center,    shift vector mu = mean of a strided sample of candidate rows (partial sums
+//   tc_center_fin per slice, then their fixed-order total and mu.mu)
 //   tc_pack       one warp per row: gather, centre, round to the MMA format into a row-major
 //                 [rows][d_pad] panel (TMA source), effective norm X2 - 2 mu.x + mu.mu (the
 //                 centred norm, built on the caller's norm) in FP64, centred norm bound, ids;
@@ -59,28 +60,37 @@ constexpr int CN_SLOTS = 3;
 // ------------------------------------------------------------------------------------------
 // shift vector
 // ------------------------------------------------------------------------------------------
-// Block of 32 warps per 32 dimensions: lane = dimension, warps stride over a strided sample of
-// the candidate rows (coalesced 128-byte row segments), then a block reduction.
+// The shift is the mean of a strided sample of the candidate rows, summed in a fixed order in
+// two steps so that it is the same bits on every run:
+//   tc_center   grid (dimension groups of 32, CENTER_SLICES slices of the sample), 32 warps per
+//               block: lane = dimension, warps stride over the slice's rows (coalesced 128-byte
+//               row segments), a block reduction in warp order, one partial sum per (slice,
+//               dimension) and one row count per slice;
+//   tc_center_fin  one block: mu = (sum of the partials in slice order) / rows, and mu.mu in FP64.
+constexpr int CENTER_SLICES = 16;
+
 __global__ void __launch_bounds__(1024) tc_center(const float *__restrict__ X, int d,
                                                   long long nrows, const int *__restrict__ idx,
                                                   int count, int nsample,
-                                                  float *__restrict__ mu) {
+                                                  double *__restrict__ part,
+                                                  int *__restrict__ part_n) {
   __shared__ double ps[32][33];
   __shared__ int pc[32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int p = blockIdx.x * 32 + lane;
+  const int t_lo = (int)((long long)nsample * blockIdx.y / CENTER_SLICES);
+  const int t_hi = (int)((long long)nsample * (blockIdx.y + 1) / CENTER_SLICES);
   double s = 0.0;
   int used = 0;
-  // eight sample rows per round: their index and row loads are independent and issue together;
-  // the sum keeps the sample order
-  for (int t0 = warp; t0 < nsample; t0 += 32 * 8) {
+  // eight sample rows per round: their index and row loads are independent and issue together
+  for (int t0 = t_lo + warp; t0 < t_hi; t0 += 32 * 8) {
     float v[8];
     bool ok[8];
 #pragma unroll
     for (int u = 0; u < 8; u++) {
       const int t = t0 + 32 * u;
       long long row = -1;
-      if (t < nsample) row = idx[(long long)t * count / nsample];
+      if (t < t_hi) row = idx[(long long)t * count / nsample];
       ok[u] = row >= 0 && row < nrows;
       v[u] = ok[u] && p < d ? X[row * d + p] : 0.0f;
     }
@@ -102,15 +112,34 @@ __global__ void __launch_bounds__(1024) tc_center(const float *__restrict__ X, i
       tot += ps[w][lane];
       n += pc[w];
     }
-    if (p < d) mu[p] = n ? (float)(tot / n) : 0.0f;
+    if (p < d) part[(size_t)blockIdx.y * d + p] = tot;
+    if (blockIdx.x == 0 && lane == 0) part_n[blockIdx.y] = n;
   }
 }
 
-__global__ void tc_mu2(const float *__restrict__ mu, int d, double *__restrict__ mu2) {
-  double s = 0.0;
-  for (int p = threadIdx.x; p < d; p += 32) s += (double)mu[p] * (double)mu[p];
-  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(FULL_MASK, s, o);
-  if (threadIdx.x == 0) *mu2 = s;
+__global__ void __launch_bounds__(256) tc_center_fin(const double *__restrict__ part,
+                                                     const int *__restrict__ part_n, int d,
+                                                     float *__restrict__ mu,
+                                                     double *__restrict__ mu2) {
+  __shared__ double red[8];
+  int n = 0;
+  for (int sl = 0; sl < CENTER_SLICES; sl++) n += part_n[sl];
+  double s2 = 0.0;
+  for (int p = threadIdx.x; p < d; p += blockDim.x) {
+    double tot = 0.0;
+    for (int sl = 0; sl < CENTER_SLICES; sl++) tot += part[(size_t)sl * d + p];
+    const float m = n ? (float)(tot / n) : 0.0f;
+    mu[p] = m;
+    s2 += (double)m * (double)m;
+  }
+  for (int o = 16; o; o >>= 1) s2 += __shfl_xor_sync(FULL_MASK, s2, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s2;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+    *mu2 = t;
+  }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1514,7 +1543,7 @@ int tc_format_of_mode(int mode) {
 
 // Prepared-candidate area: mu, mu2, stats, panel(s), norms, norm bounds, ids.
 struct CandLayout {
-  size_t o_mu, o_mu2, o_stats, o_pb, o_pb_lo, o_pn, o_cn, o_cnrm, o_cid, bytes;
+  size_t o_mu, o_mu2, o_cpart, o_stats, o_pb, o_pb_lo, o_pn, o_cn, o_cnrm, o_cid, bytes;
   int fmt, elem, d_pad, r_pad;
 };
 
@@ -1530,6 +1559,7 @@ static CandLayout cand_layout(int nc, int d, int mode) {
   auto take = [&](size_t b) { size_t o = off; off = al256(off + b); return o; };
   L.o_mu = take((size_t)d * 4);
   L.o_mu2 = take(8);
+  L.o_cpart = take((size_t)CENTER_SLICES * d * 8 + CENTER_SLICES * 4);
   L.o_stats = take(16);
   L.o_pb = take((size_t)L.r_pad * L.d_pad * L.elem);
   L.o_pb_lo = L.fmt == 2 ? take((size_t)L.r_pad * L.d_pad * L.elem) : 0;
@@ -1564,8 +1594,13 @@ cudaError_t tc_cand_prepare(TcCand *C, void *mem, int nc, int d, int mode, const
   cudaError_t e = cudaMemsetAsync(C->stats, 0, 16, st);
   if (e != cudaSuccess) return e;
   const int nsample = std::min(nc, 4096);
-  tc_center<<<(d + 31) / 32, 1024, 0, st>>>(Xc, d, nrows_c, cidx, nc, nsample, C->mu);
-  tc_mu2<<<1, 32, 0, st>>>(C->mu, d, C->mu2);
+  {
+    double *part = reinterpret_cast<double *>(base + L.o_cpart);
+    int *part_n = reinterpret_cast<int *>(base + L.o_cpart + (size_t)CENTER_SLICES * d * 8);
+    tc_center<<<dim3((d + 31) / 32, CENTER_SLICES), 1024, 0, st>>>(Xc, d, nrows_c, cidx, nc,
+                                                                    nsample, part, part_n);
+    tc_center_fin<<<1, 256, 0, st>>>(part, part_n, d, C->mu, C->mu2);
+  }
   tc_pack<<<tc_pack_grid(L.r_pad), 256, 0, st>>>(L.fmt, Xc, Xc2, d, L.d_pad, nrows_c, cidx, nc,
                                             L.r_pad, C->mu, C->mu2, 1, C->pb, C->pb_lo, C->cn,
                                             C->cnrm, C->cid, C->stats, status, nullptr, nullptr,
@@ -1980,6 +2015,7 @@ TcLeafPlan tc_leaf_plan(long long npts, int rows_cap, int d, int k, int sms) {
   const size_t R = (size_t)L.rows_cap;
   L.o_mu = take((size_t)d * 4);
   L.o_mu2 = take(8);
+  L.o_cpart = take((size_t)CENTER_SLICES * d * 8 + CENTER_SLICES * 4);
   L.o_stats = take(16);
   L.o_pb = take(R * P.d_pad * 2);
   L.o_pb_lo = take(R * P.d_pad * 2);
@@ -2035,9 +2071,11 @@ cudaError_t tc_leaf_pass(const TcLeafPlan &L, void *ws, const float *X, const fl
     // once per workspace: the row index map, and the shift (mean of a strided sample of the
     // first panel's rows, padding skipped), which serves every later tree of the same table
     iota_kernel<<<296, 256, 0, st>>>(iota, npts);
-    tc_center<<<(d + 31) / 32, 1024, 0, st>>>(X, d, npts, pidx, rows, std::min(rows, 4096),
-                                              mu);
-    tc_mu2<<<1, 32, 0, st>>>(mu, d, mu2);
+    double *part = reinterpret_cast<double *>(base + L.o_cpart);
+    int *part_n = reinterpret_cast<int *>(base + L.o_cpart + (size_t)CENTER_SLICES * d * 8);
+    tc_center<<<dim3((d + 31) / 32, CENTER_SLICES), 1024, 0, st>>>(
+        X, d, npts, pidx, rows, std::min(rows, 4096), part, part_n);
+    tc_center_fin<<<1, 256, 0, st>>>(part, part_n, d, mu, mu2);
   }
   tc_pack<<<tc_pack_grid(rows), 256, 0, st>>>(2, X, X2, d, P.d_pad, npts, pidx, rows, rows, mu, mu2,
                                          1, pb, pb_lo, cn, cnrm, cid, stats, status, nullptr,
