@@ -1131,10 +1131,13 @@ __device__ __forceinline__ void rerank_body(const RerankParams &p) {
     for (int s = 0; s < p.S; s++) {
       const int cnt = p.logcnt[(size_t)s * p.Q + q];
       const uint2 *lg = p.log + ((size_t)s * p.Q + q) * p.logcap;
+      // one batch of log entries is loaded ahead, so that its latency overlaps the vote and
+      // merge of the current batch
+      float dv_next = lane < cnt ? __uint_as_float(lg[lane].x) : Num<float>::inf();
       for (int base = 0; base < cnt; base += 32) {
         const int e = base + lane;
-        float dv = Num<float>::inf();
-        if (e < cnt) dv = __uint_as_float(lg[e].x);
+        const float dv = dv_next;
+        dv_next = e + 32 < cnt ? __uint_as_float(lg[e + 32].x) : Num<float>::inf();
         if (!__any_sync(FULL_MASK, dv <= kth)) continue;
         float b1[1] = {dv};
         uint32_t i1[1] = {(uint32_t)e};
