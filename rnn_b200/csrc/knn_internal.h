@@ -101,7 +101,8 @@ typedef void (*TraceHook)(void *ctx, const char *name, bool begin, cudaStream_t 
                           int nkernels);
 
 // Epilogue warps of the tensor-core kernel: TC_EPI_WARPS / 4 per TMEM lane quarter, each with its
-// own band log per (query, split); the first warp of a quarter keeps the row's heap.
+// own band log per (query, split) and its own heap of ceil(k/2) entries per row (the partition
+// bound).
 constexpr int TC_EPI_WARPS = 8;
 constexpr int TC_EPI_PARTS = TC_EPI_WARPS / 4;
 

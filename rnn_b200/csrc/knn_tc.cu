@@ -12,14 +12,19 @@
 //                 centred norm, built on the caller's norm) in FP64, centred norm bound, ids;
 //                 running maxima for the bound
 //   tc_knn        warp 0 TMA producer, warp 1 MMA issuer (TMEM owner), warps 2-9 epilogue (two
-//                 per TMEM lane quarter, each taking half of every tile's columns) with
-//                 one query row per thread: approximate d' = qn' + cn' - 2<q~,c~>; per row and
-//                 epilogue part a max-heap of the hk smallest d' of its own columns in shared
-//                 memory, where hk = ceil(k / (parts in a window of up to 4 splits)), so that the
-//                 largest root of a window bounds the k-th from above (threshold = that + 2E);
-//                 a per-query log in HBM of every candidate under the threshold
+//                 per TMEM lane quarter, each taking half of every tile's columns) with one
+//                 query row per thread: approximate d' = qn' + cn' - 2<q~,c~> (with the norm
+//                 column, cn' enters through one extra MMA against an all-ones A tile and the
+//                 accumulator holds w = -v/2); per row and epilogue part a max-heap of the
+//                 ceil(k/2) smallest d' of its own columns in shared memory; any two such heaps
+//                 hold k candidates, so the second smallest root a row can see (its own, the
+//                 other part's, and the roots up to three other splits published) bounds the
+//                 k-th from above (threshold = that + 2E); a per-query log in HBM of every
+//                 candidate under the threshold
 //   tc_rerank     one warp per query: exact FP64 distances of the logged band, sorted merge with
-//                 the incoming heap row, descending write-back (a valid max-heap)
+//                 the incoming heap row, descending write-back (a valid max-heap);
+//                 tc_rerank_hold (BF16, k <= 64) holds the band above the approximate k-th back,
+//                 tc_rerank_leaf (batching form) sorts and writes a row only if it changes
 //   tc_fallback   queries whose log overflowed: exact FP64 brute force over all candidates
 //
 // Error bound (per query q, all candidates c; u = unit roundoff of the MMA input format,
@@ -27,7 +32,8 @@
 //   |d'(q,c) - d(q,c)| <= E_q = 1.25 * [ 2 (2u + u^2 + D 2^-23 (1+u)^2) |q~| M
 //                                         + 3 * 2^-24 (CN + |qn'| + 2 |q~| M) ]
 // For the split format the input term 2u + u^2 is replaced by 3.2 u^2 (u = 2^-8) and the
-// accumulation term counts 3D products.
+// accumulation term counts 3D products. With the norm column the accumulation counts 3 more
+// terms, and E gains 1.25 (n 2^-23 + 2^-24) CN for the norm parts it sums (n accumulated terms).
 #include "knn_common.cuh"
 #include "knn_internal.h"
 #include "tc_ptx.cuh"
